@@ -1,0 +1,373 @@
+#!/usr/bin/env python3
+"""Benchmark of the per-trial Monte Carlo path on B200.
+
+Workload (a "step"): one batch of 2^20 trials of the plain GPU configuration
+N = 2^20 keys (ell_i 20), t = 1024 items, k = 3, B = 1536 buckets, max 500
+kicks, BGH25 random walk, affine distinct inputs, seed 2, BT = 20.  Step s on
+rank r evaluates batch r + s*N_ranks, so every step is new work.
+
+Prints one JSON line (rank 0).  `value` is whole-job trials/s from CUDA
+events around the engine launches on device-resident inputs; `e2e` is the same
+metric through the C ABI call cmc_launch with host buffers (batch key in,
+sorted failure offsets out, copies inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "pbc-based-dmpf-monte-carlo-test_b200"
+
+WORKLOAD = dict(workload="plain GPU: N=2^20 keys, t=1024, k=3, B=1536, kick=500, bgh25, "
+                         "affine inputs, seed 2, batches of 2^20 trials",
+                mode="bgh25", input_mode="affine", pnum=1024, ell_i=20, k=3, buckets=1536,
+                kick=500, seed=2, bt=20)
+METRIC = "trials/s per B200 (bit-exact failures)"
+AES_BYTES_PER_BLOCK = 640      # 160 table lookups x 4 bytes
+SMEM_BYTES_PER_CLK_PER_SM = 128
+
+
+def load_pkg():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("cmc_b200", PKG_DIR / "__init__.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["cmc_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def algorithmic_blocks(p) -> float:
+    """A = 2 + min(8*2^h, ceil(8*k*t*c)) AES blocks per trial, c = 2^(2h)/D."""
+    c = (2.0 ** (2 * p.half_bits)) / p.domain
+    return 2 + min(8 * 2 ** p.half_bits, math.ceil(8 * p.k * p.pnum * c))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_peaks() -> dict:
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def read_traffic() -> float | None:
+    """DRAM bytes per engine launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "engine_config2_traffic.txt"
+    try:
+        for line in f.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch"):
+                return float(line.split("=")[1])
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
+
+
+# ------------------------------------------------------------- CPU baseline --
+
+def reference_lib():
+    path = ROOT / "oracle" / "_ref" / "libcmcref.so"
+    if not path.exists():
+        return None
+    lib = ctypes.CDLL(str(path))
+    u32, u64 = ctypes.c_uint32, ctypes.c_uint64
+    lib.ref_batch_launch.argtypes = [ctypes.c_char_p, ctypes.c_char_p, u32, u32, u32, u32, u64,
+                                     u64, u32, ctypes.c_int, ctypes.POINTER(u32),
+                                     ctypes.POINTER(ctypes.c_int)]
+    lib.ref_batch_launch.restype = u32
+    lib.ref_has_aesni.restype = ctypes.c_int
+    return lib if lib.ref_has_aesni() else None
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_run(n_trials: int, batch: int, threads: int):
+    """Trials [0, n) of `batch` on the CPU: the reference's own cpu_batch_launch
+    (oracle/_ref) when built here, else the oracle restatement.  Returns
+    (seconds, kind, failures)."""
+    w = WORKLOAD
+    lib = reference_lib()
+    out = (ctypes.c_uint32 * max(n_trials, 1))()
+    t0 = time.perf_counter()
+    if lib is not None:
+        used = ctypes.c_int()
+        n = lib.ref_batch_launch(w["mode"].encode(), w["input_mode"].encode(), w["pnum"],
+                                 w["ell_i"], w["buckets"], w["kick"], w["seed"], batch, n_trials,
+                                 threads, out, ctypes.byref(used))
+        kind = "reference"
+    else:
+        sys.path.insert(0, str(ROOT / "tests"))
+        from oracle_binding import Oracle
+        o = Oracle()
+        p = o.params(w["mode"], w["pnum"], w["ell_i"], w["k"], w["buckets"], w["kick"],
+                     w["input_mode"])
+        n = len(o.batch(p, w["seed"], batch, 0, n_trials, threads))
+        kind = "port"
+    return time.perf_counter() - t0, kind, n
+
+
+def cpu_baseline(target_seconds: float = 10.0) -> dict:
+    threads = host_threads()
+    secs, kind, _ = cpu_run(max(64, threads * 8), 0, threads)
+    rate = max(64, threads * 8) / max(secs, 1e-6)
+    n = int(min(1 << 20, max(256, rate * target_seconds)))
+    secs, kind, _ = cpu_run(n, 0, threads)
+    return {"value": n / secs, "unit": "trials/s", "cores": threads, "kind": kind,
+            "sample": f"first {n} trials of batch 0 of the bench workload "
+                      f"({'reference cpu_batch_launch, AES-NI' if kind == 'reference' else 'oracle port'}, "
+                      f"{threads} threads, {secs:.1f} s)"}
+
+
+def run_reference_arm(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    threads = host_threads()
+    w = WORKLOAD
+    # bounded sample per step, sized from a short probe (~1 s per step)
+    secs, kind, _ = cpu_run(max(64, threads * 8), 0, threads)
+    per_step = int(min(1 << 20, max(128, (max(64, threads * 8) / max(secs, 1e-6)) * 1.0)))
+    for s in range(args.warmup):
+        cpu_run(per_step, s, threads)
+    total = 0.0
+    for s in range(args.steps):
+        secs, kind, _ = cpu_run(per_step, args.warmup + s, threads)
+        total += secs
+    value = per_step * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "trials/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded AES-CTR trial stream)",
+        "config": {"workload": w["workload"], "trials_per_step": per_step,
+                   "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": "trials/s", "cores": threads, "kind": kind,
+                         "sample": f"{per_step} trials per step, batches {args.warmup}.."
+                                   f"{args.warmup + args.steps - 1}"},
+        "e2e": {"value": value, "unit": "trials/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm --
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    cmc = load_pkg()
+    ctx = cmc.Context(local)
+    w = WORKLOAD
+    p = cmc.parameters(w["mode"], w["pnum"], w["ell_i"], w["k"], w["buckets"], w["kick"],
+                       w["input_mode"])
+    n = 1 << w["bt"]
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    d_out = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_n = torch.zeros(1, dtype=torch.int32, device="cuda")
+    keys = {}
+
+    def key_of(batch):
+        if batch not in keys:
+            keys[batch] = torch.tensor(cmc.batch_key(w["seed"], batch), dtype=torch.int64) \
+                .to(torch.int32).cuda()
+        return keys[batch]
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def batch_of(step):
+        return rank + world * step
+
+    # warm-up (untimed)
+    for s in range(args.warmup):
+        ctx.launch_device(p, key_of(batch_of(s)).data_ptr(), 0, n, d_out.data_ptr(),
+                          d_n.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    ctx.check()
+
+    # timed region: K steps, per-step events on the launching stream, L2 flushed between
+    steps = list(range(args.warmup, args.warmup + args.steps))
+    for s in steps:
+        key_of(batch_of(s))
+    starts = [torch.cuda.Event(enable_timing=True) for _ in steps]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in steps]
+    engine_ms = []
+    failures = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for i, s in enumerate(steps):
+            flush.zero_()
+            starts[i].record(stream)
+            ctx.launch_device(p, key_of(batch_of(s)).data_ptr(), 0, n, d_out.data_ptr(),
+                              d_n.data_ptr(), stream.cuda_stream)
+            ends[i].record(stream)
+            engine_ms.append(ctx.last_engine_ms())
+            failures += int(d_n.item())
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ctx.check()
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    launches = ctx.last_kernel_count * len(steps)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * n * len(steps) / (max_ms / 1e3)
+
+    # e2e: the C ABI call with host buffers, copies inside the timed region
+    e2e_steps = list(range(args.warmup + args.steps, args.warmup + 2 * args.steps))
+    host_keys = {s: cmc.batch_key(w["seed"], batch_of(s)) for s in e2e_steps}
+    ctx.launch(p, host_keys[e2e_steps[0]], 0, n)  # warm host path
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    d2h = 0
+    for s in e2e_steps:
+        fails = ctx.launch(p, host_keys[s], 0, n)
+        d2h += 4 + 4 * len(fails)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * len(e2e_steps) / (float(t.item()) / 1e3)
+
+    if rank == 0:
+        peaks = read_peaks()
+        clk = clocks.summary()
+        blocks = algorithmic_blocks(p)
+        mean_engine_ms = statistics.mean(engine_ms)
+        achieved = blocks * AES_BYTES_PER_BLOCK * n / (mean_engine_ms / 1e3) / 1e9
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        max_mhz = peaks.get("sm_max_mhz") or clk.get("sm_max_mhz") or 1965.0
+        peak = sms * SMEM_BYTES_PER_CLK_PER_SM * max_mhz * 1e6 / 1e9
+        traffic = read_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": world,
+            "steps": len(steps), "warmup": args.warmup, "ms_per_step": max_ms / len(steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded AES-CTR trial stream; no dataset)",
+            "config": {"workload": w["workload"], "trials_per_step": n,
+                       "parallelism": f"replicas x{world} (disjoint batches, no collective)",
+                       "l2": "256 MiB buffer written between steps, outside the step events",
+                       "plan": ctx.last_plan},
+            "e2e": {"value": e2e_value, "unit": "trials/s", "h2d_bytes_per_step": 176,
+                    "d2h_bytes_per_step": d2h // len(e2e_steps)},
+            "gpu_launches": launches,
+            "failures_in_timed_steps": failures,
+            "roofline": {
+                "bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "basis": f"A={blocks:.0f} AES blocks/trial x 640 B of T-table lookups; peak = "
+                         f"{sms} SMs x 128 B/clk x {max_mhz:.0f} MHz (sm_max_mhz of "
+                         f"MEASURED_PEAKS.json); engine kernel {mean_engine_ms:.2f} ms/launch",
+            },
+            "clocks": clk,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,118 @@
+/*
+ * cmc.h -- C ABI of the B200 cuckoo-hashing Monte Carlo estimator (libcmc.so).
+ *
+ * The reference has no plugin layer; its replaceable seam is the Launch
+ * callable that process_batch() invokes (cuckoo_bench.cu:724-736):
+ *     launch(uint32_t n, uint32_t offset, const AesKey& batch_key,
+ *            std::vector<uint32_t>& failures)
+ * cmc_launch() is that seam as a C function: plain pointers and sizes, no
+ * C++ or torch types.  Everything else here is the state the reference keeps
+ * around that call (device set-up, parameters, batch keys) plus the batched
+ * and served forms of the same computation.
+ *
+ * All functions return 0 on success or a negative CMC_E* code; they never
+ * throw.  cmc_last_error() gives the message of the last failure on a
+ * context (or on the calling thread when ctx is NULL).
+ */
+#ifndef CMC_H
+#define CMC_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMC_OK 0
+#define CMC_EINVAL (-1)       /* invalid argument or unsupported parameters   */
+#define CMC_ECUDA (-2)        /* CUDA runtime error                           */
+#define CMC_EKAT (-3)         /* device AES known-answer test failed          */
+#define CMC_ETIMEOUT (-4)     /* a bounded device wait gave up                */
+#define CMC_ERANGE (-5)       /* device result out of range (nf > n)          */
+#define CMC_ENOMEM (-6)       /* allocation failed                            */
+
+#define CMC_MODE_BGH25 1u     /* random-walk eviction (cuckoo_core.hpp:123-133) */
+#define CMC_MODE_DRRT18 2u    /* cycling eviction     (cuckoo_core.hpp:134-158) */
+#define CMC_INPUT_SEQUENTIAL 0u
+#define CMC_INPUT_AFFINE 1u
+
+/* Derived experiment parameters.  Mirrors Options+Params of the reference
+ * (cuckoo_bench.cu:406-419, 499-526) with the copy count k generalised. */
+typedef struct cmc_params {
+    uint32_t mode;        /* CMC_MODE_*                                   */
+    uint32_t input_mode;  /* CMC_INPUT_*                                  */
+    uint32_t pnum;        /* t, items per trial, 3..65534                 */
+    uint32_t ell_i;       /* key domain 2^ell_i, ell_i <= 61              */
+    uint32_t k;           /* hash copies, 2..4 (reference: 3)             */
+    uint32_t buckets;     /* B                                            */
+    uint32_t kick;        /* eviction limit                               */
+    uint32_t half_bits;   /* Feistel half width h                         */
+    uint64_t bucket_size; /* ceil(k * 2^ell_i / B)                        */
+    uint64_t domain;      /* D = B * bucket_size                          */
+    uint64_t mask;        /* 2^h - 1                                      */
+    uint64_t range_mask;  /* 2^ell_i - 1                                  */
+} cmc_params;
+
+/* parameters() (cuckoo_bench.cu:483-526), k-generalised; a zero override
+ * keeps the reference derivation of B (resp. the eviction limit). */
+int cmc_derive_params(uint32_t mode, uint32_t pnum, uint32_t ell_i, uint32_t k,
+                      uint32_t buckets_override, uint32_t kick_override,
+                      uint32_t input_mode, cmc_params* out);
+
+/* batch_key(seed, batch_id) (cuckoo_bench.cu:393-404): the 44-word AES-128
+ * key schedule of one batch. */
+void cmc_batch_key(uint64_t seed, uint64_t batch_id, uint32_t out_w[44]);
+
+/* Host AES-128 of one block under a 44-word schedule (cuckoo_bench.cu:360-392). */
+void cmc_host_aes128(const uint32_t rk[44], const uint32_t in[4], uint32_t out[4]);
+
+typedef struct cmc_ctx cmc_ctx;
+
+/* Per-device set-up: table upload and the FIPS-197 known-answer test on the
+ * device (cuckoo_bench.cu:1090-1095, 332-354).  One context per host thread. */
+int cmc_init(int device, cmc_ctx** out);
+int cmc_destroy(cmc_ctx* ctx);
+const char* cmc_last_error(const cmc_ctx* ctx);
+
+/* The Launch seam (cuckoo_bench.cu:980-1031): evaluate trials
+ * [first, first+count) of the batch whose key schedule is batch_key (host
+ * memory), append nothing and instead write the failing within-batch
+ * offsets, ascending, to out_offsets (host memory, capacity count) and their
+ * number to *out_nfailed.  Synchronous, like the reference. */
+int cmc_launch(cmc_ctx* ctx, const cmc_params* params, const uint32_t batch_key[44],
+               uint32_t first, uint32_t count, uint32_t* out_offsets, uint32_t* out_nfailed);
+
+/* Device-resident form of cmc_launch: batch_key, out_offsets (capacity count)
+ * and out_nfailed are device pointers; work is queued on `stream`
+ * (cudaStream_t, NULL = the context's stream) and the call returns without
+ * waiting.  cmc_check() afterwards reports bounded-wait timeouts. */
+int cmc_launch_device(cmc_ctx* ctx, const cmc_params* params, const uint32_t* d_batch_key,
+                      uint32_t first, uint32_t count, uint32_t* d_out_offsets,
+                      uint32_t* d_out_nfailed, void* stream);
+int cmc_check(cmc_ctx* ctx);
+
+/* Tuning knobs of the launch planner; value 0 (or -1 for "method") restores
+ * the automatic choice.  Names: "warps_per_group" (1..15), "groups" (1..14),
+ * "global_slots" (0/1: keep walk slots in global memory), "method"
+ * (-1 auto, 0 direct AES passes, 1 shared-memory round cache), "spin_limit"
+ * (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown
+ * name or a value out of range. */
+int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
+
+/* Queue this context's host-buffer launches (cmc_launch) on `stream`
+ * (cudaStream_t; NULL restores the context's own stream). */
+int cmc_set_stream(cmc_ctx* ctx, void* stream);
+
+/* Device time of the last engine kernel (CUDA events around that one
+ * launch), in milliseconds; waits for it to finish.  -1 on error. */
+double cmc_last_engine_ms(cmc_ctx* ctx);
+
+/* Kernels launched by the last cmc_launch* call on this context. */
+uint32_t cmc_last_kernel_count(const cmc_ctx* ctx);
+/* Human-readable description of the last launch plan (engine, groups, ...). */
+const char* cmc_last_plan(const cmc_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

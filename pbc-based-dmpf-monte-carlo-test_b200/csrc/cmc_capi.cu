@@ -1,0 +1,449 @@
+// cmc_capi.cu -- C ABI over the engine: per-device context, launch planning
+// and the Launch seam (cuckoo_bench.cu:980-1031).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cmc.h"
+#include "cmc_capi_internal.hpp"
+#include "cmc_engine.cuh"
+#include "cmc_hostcore.hpp"
+
+namespace cmc {
+
+template <typename MapT, typename BinT, bool WIDE>
+__global__ void cmc_engine(const EngineArgs a);
+__global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
+                                     uint32_t* out, uint32_t* count);
+__global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out);
+
+namespace {
+
+thread_local std::string g_thread_error;
+
+constexpr uint32_t kCtaSharedBytes = 2048;
+constexpr uint32_t kGroupHeaderBytes = 512;
+
+uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+int Ctx::fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+}
+
+int Ctx::cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CMC_OK;
+    return fail(CMC_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+template <typename T>
+int Ctx::grow(T*& ptr, size_t& cap, size_t need, const char* what) {
+    if (need <= cap && ptr) return CMC_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    size_t n = std::max<size_t>(need, 1);
+    if (cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CMC_ENOMEM, "cudaMalloc of %zu bytes for %s failed", n * sizeof(T), what);
+    }
+    cap = n;
+    return CMC_OK;
+}
+
+// Fill a device job descriptor from derived parameters.
+int Ctx::make_job(const cmc_params& p, uint32_t first, uint32_t count, uint64_t base, Job& j) {
+    std::memset(&j, 0, sizeof j);
+    if (p.mode != CMC_MODE_BGH25 && p.mode != CMC_MODE_DRRT18)
+        return fail(CMC_EINVAL, "invalid mode %u", p.mode);
+    if (p.k < 2 || p.k > 4) return fail(CMC_EINVAL, "k must be 2..4 (got %u)", p.k);
+    if (p.pnum < 3 || p.pnum > 65534) return fail(CMC_EINVAL, "PNUM out of range");
+    if (p.buckets < 1 || p.bucket_size < 1 || p.domain == 0)
+        return fail(CMC_EINVAL, "invalid bucket parameters");
+    if (p.domain > 0xffffffffULL) {
+        if (p.half_bits > 32) return fail(CMC_EINVAL, "PRP half width above 32 bits");
+    } else if (p.half_bits > 16) {
+        return fail(CMC_EINVAL, "PRP half width inconsistent with domain");
+    }
+    if (uint64_t(p.pnum) * p.k > 0xffffffffULL) return fail(CMC_EINVAL, "too many candidates");
+    j.pnum = p.pnum;
+    j.k = p.k;
+    j.buckets = p.buckets;
+    j.kick = p.kick;
+    j.mode = p.mode;
+    j.input_mode = p.input_mode;
+    j.half_bits = p.half_bits;
+    j.domain = p.domain;
+    j.mask = p.mask;
+    j.range_mask = p.range_mask;
+    j.width = p.bucket_size;
+    j.width_magic = p.domain <= 0xffffffffULL ? uint32_t(0xffffffffULL / p.bucket_size) : 0;
+    j.first = first;
+    j.count = count;
+    j.trial_base = base;
+    // Round cache when it costs fewer AES blocks than direct passes and fits
+    // a group's shared memory (8 * 2^h u16 entries, h <= 12).
+    const double c = std::ldexp(1.0, 2 * int(p.half_bits)) / double(p.domain);
+    const double direct = double(p.pnum) * p.k * 8.0 * c;
+    const double cache = 8.0 * std::ldexp(1.0, int(p.half_bits)) + direct / 64.0;
+    j.method = (p.half_bits <= 12 && cache < direct && force_method != 0) ? kMethodCache : kMethodDirect;
+    if (force_method == 1 && p.half_bits <= 12) j.method = kMethodCache;
+    return CMC_OK;
+}
+
+// Choose groups, warps per group and slot placement for a set of jobs.
+int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
+    uint32_t max_b = 0, max_cand = 0, max_cache_h = 0, any_cache = 0, wide = 0, wide_domain = 0;
+    double work = 0, cand_work = 0;
+    for (const Job& j : jobs) {
+        max_b = std::max(max_b, j.buckets);
+        max_cand = std::max(max_cand, j.pnum * j.k);
+        if (j.method == kMethodCache) {
+            any_cache = 1;
+            max_cache_h = std::max(max_cache_h, j.half_bits);
+        }
+        if (j.domain > 0xffffffffULL) wide_domain = 1;
+        // 16-bit entries: 14-bit ordinal + 2-bit choice, never equal to 0xffff
+        const bool narrow_ok = j.buckets <= 0xffff && j.pnum <= 16384 && !(j.k == 4 && j.pnum > 16383);
+        if (!narrow_ok) wide = 1;
+        work += double(j.count);
+        cand_work += double(j.count) * j.pnum * j.k;
+    }
+    if (wide_domain) wide = 1;
+    pl.variant = wide_domain ? 2 : (wide ? 1 : 0);
+    const uint32_t entry = wide ? 4 : 2;
+    pl.bins_bytes = round_up(max_b * entry, 16);
+    const uint32_t map_bytes = round_up(max_cand * entry, 16);
+    pl.slot_stride = round_up(pl.bins_bytes + map_bytes, 128);
+    const uint32_t cache_bytes = any_cache ? (16u << max_cache_h) : 0;
+    pl.group_bytes = kGroupHeaderBytes + cache_bytes;
+    const double avg_cand = work > 0 ? cand_work / work : 0;
+    pl.wg = (any_cache || avg_cand >= 768.0) ? 4 : 1;
+    if (force_wg) pl.wg = force_wg;
+    const uint32_t max_producer_warps = 15;
+    const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
+    uint32_t ng = std::min<uint32_t>(kMaxGroups, max_producer_warps / pl.wg);
+    if (force_ng) ng = std::min(ng, force_ng);
+    while (ng > 1 && ng * pl.group_bytes > budget) --ng;
+    if (ng * pl.group_bytes > budget)
+        return fail(CMC_EINVAL, "round cache of %u bytes does not fit shared memory", cache_bytes);
+    // Slots: 2..4 per group in shared memory when that fits without giving up
+    // more than half of the groups; otherwise up to 32 in global memory.
+    pl.slots_smem = false;
+    for (uint32_t g = ng; !force_global_slots && g >= std::max<uint32_t>(1, (ng + 1) / 2); --g) {
+        const uint32_t left = budget - g * pl.group_bytes;
+        const uint32_t s = std::min<uint32_t>({left / pl.slot_stride / g, kMaxSlots / g, 4u});
+        if (s >= 2) {
+            pl.ng = g;
+            pl.ns = g * s;
+            pl.slots_smem = true;
+            break;
+        }
+    }
+    if (!pl.slots_smem) {
+        pl.ng = ng;
+        pl.ns = std::max<uint32_t>(1, kMaxSlots / ng) * ng;
+    }
+    pl.group_off = kEngineTableBytes + kCtaSharedBytes;
+    pl.slots_off = pl.group_off + pl.ng * pl.group_bytes;
+    pl.smem_bytes = pl.slots_off + (pl.slots_smem ? pl.ns * pl.slot_stride : 0);
+    pl.threads = (pl.ng * pl.wg + 1) * 32;
+    pl.ctas = sms;
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "engine=group variant=%s groups=%u warps_per_group=%u slots=%u slots_in=%s "
+             "smem=%u threads=%u ctas=%u cache=%s",
+             pl.variant == 0 ? "narrow" : pl.variant == 1 ? "wide" : "wide-domain", pl.ng, pl.wg,
+             pl.ns, pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
+             any_cache ? "on" : "off");
+    plan_text = buf;
+    return CMC_OK;
+}
+
+// Queue one engine launch over `jobs` (already on the device in d_jobs) and
+// the compaction of its failure bitmap.
+int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint32_t value_base,
+             uint32_t* d_out, uint32_t* d_count, unsigned long long* job_failed,
+             unsigned long long* job_done) {
+    Plan pl;
+    int rc = plan(jobs, pl);
+    if (rc) return rc;
+    const size_t words = (total + 31) / 32;
+    if ((rc = grow(d_bits, bits_cap, words, "failure bitmap"))) return rc;
+    if (!pl.slots_smem) {
+        const size_t need = size_t(pl.ctas) * pl.ns * pl.slot_stride;
+        if ((rc = grow(d_slots, slots_cap, need, "slot pool"))) return rc;
+    }
+    if ((rc = cuda(cudaMemsetAsync(d_ctrl, 0, sizeof(Ctrl), st), "memset ctrl"))) return rc;
+    if ((rc = cuda(cudaMemsetAsync(d_bits, 0, words * 4, st), "memset bitmap"))) return rc;
+    EngineArgs a{};
+    a.jobs = d_jobs;
+    a.njobs = uint32_t(jobs.size());
+    a.total = total;
+    a.ctrl = d_ctrl;
+    a.fail_bits = d_bits;
+    a.job_failed = job_failed;
+    a.job_done = job_done;
+    a.gslots = pl.slots_smem ? nullptr : d_slots;
+    a.t0 = d_t0;
+    a.slot_stride = pl.slot_stride;
+    a.bins_bytes = pl.bins_bytes;
+    a.ng = pl.ng;
+    a.wg = pl.wg;
+    a.ns = pl.ns;
+    a.group_bytes = pl.group_bytes;
+    a.group_off = pl.group_off;
+    a.slots_off = pl.slots_off;
+    a.spin_limit = spin_limit;
+    const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
+                   : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
+                                     : (const void*)cmc_engine<uint32_t, uint32_t, true>;
+    if ((rc = cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(pl.smem_bytes)),
+                   "cudaFuncSetAttribute")))
+        return rc;
+    void* args[] = {&a};
+    if ((rc = cuda(cudaEventRecord(ev_start, st), "event"))) return rc;
+    if ((rc = cuda(cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, st),
+                   "engine launch")))
+        return rc;
+    if ((rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
+    kernels = 1;
+    if (d_out) {
+        cmc_compact_failures<<<1, 1024, 0, st>>>(d_bits, total, value_base, d_out, d_count);
+        if ((rc = cuda(cudaGetLastError(), "compaction launch"))) return rc;
+        kernels = 2;
+    }
+    last_plan = pl;
+    return CMC_OK;
+}
+
+int Ctx::check_ctrl() {
+    Ctrl c{};
+    int rc = cuda(cudaMemcpy(&c, d_ctrl, sizeof c, cudaMemcpyDeviceToHost), "read ctrl");
+    if (rc) return rc;
+    last_walks = c.walks;
+    last_probes = c.probes;
+    if (c.error)
+        return fail(-int(c.error), "device wait gave up (site %u): results discarded", c.where);
+    return CMC_OK;
+}
+
+int Ctx::init(int dev) {
+    device = dev;
+    int rc = cuda(cudaSetDevice(dev), "cudaSetDevice");
+    if (rc) return rc;
+    cudaDeviceProp prop{};
+    if ((rc = cuda(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties"))) return rc;
+    if (prop.major < 10)
+        return fail(CMC_EINVAL, "device %d (%s, sm_%d%d) is not an sm_100 GPU", dev, prop.name,
+                    prop.major, prop.minor);
+    sms = prop.multiProcessorCount;
+    smem_optin = prop.sharedMemPerBlockOptin;
+    if ((rc = cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream"))) return rc;
+    if ((rc = cuda(cudaEventCreate(&ev_start), "event"))) return rc;
+    if ((rc = cuda(cudaEventCreate(&ev_stop), "event"))) return rc;
+    uint32_t t0[256];
+    t0_table(t0);
+    size_t cap = 0;
+    if ((rc = grow(d_t0, cap, 256 + 44 + 32, "tables"))) return rc;
+    uint32_t fips[44];
+    expand_u64(0x0706050403020100ULL, 0x0f0e0d0c0b0a0908ULL, fips);
+    if ((rc = cuda(cudaMemcpy(d_t0, t0, sizeof t0, cudaMemcpyHostToDevice), "upload T0"))) return rc;
+    if ((rc = cuda(cudaMemcpy(d_t0 + 256, fips, sizeof fips, cudaMemcpyHostToDevice), "upload KAT key")))
+        return rc;
+    size_t c1 = 0;
+    if ((rc = grow(d_ctrl, c1, 1, "ctrl"))) return rc;
+    const uint32_t kat_smem = kEngineTableBytes;
+    if ((rc = cuda(cudaFuncSetAttribute((const void*)cmc_selftest,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kat_smem),
+                   "selftest attribute")))
+        return rc;
+    cmc_selftest<<<1, 32, kat_smem, stream>>>(d_t0, d_t0 + 256, d_t0 + 300);
+    if ((rc = cuda(cudaGetLastError(), "selftest launch"))) return rc;
+    uint32_t bad[32];
+    if ((rc = cuda(cudaMemcpyAsync(bad, d_t0 + 300, sizeof bad, cudaMemcpyDeviceToHost, stream),
+                   "selftest read")))
+        return rc;
+    if ((rc = cuda(cudaStreamSynchronize(stream), "selftest sync"))) return rc;
+    for (int i = 0; i < 32; ++i)
+        if (bad[i]) return fail(CMC_EKAT, "device AES known-answer test failed (lane %d, flags %u)", i, bad[i]);
+    return CMC_OK;
+}
+
+Ctx::~Ctx() {
+    if (device >= 0) cudaSetDevice(device);
+    cudaFree(d_t0);
+    cudaFree(d_ctrl);
+    cudaFree(d_jobs);
+    cudaFree(d_bits);
+    cudaFree(d_out);
+    cudaFree(d_slots);
+    cudaFree(d_key);
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_stop) cudaEventDestroy(ev_stop);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int Ctx::upload_jobs(const std::vector<Job>& jobs, cudaStream_t st) {
+    int rc = grow(d_jobs, jobs_cap, jobs.size(), "job table");
+    if (rc) return rc;
+    return cuda(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(Job),
+                                cudaMemcpyHostToDevice, st),
+                "upload jobs");
+}
+
+int Ctx::launch_host(const cmc_params& p, const uint32_t key[44], uint32_t first, uint32_t count,
+                     uint32_t* out, uint32_t* nfailed) {
+    kernels = 0;
+    if (!key || !out || !nfailed) return fail(CMC_EINVAL, "null argument");
+    *nfailed = 0;
+    if (count == 0) return CMC_OK;
+    if (uint64_t(first) + count > 0x100000000ULL) return fail(CMC_EINVAL, "offset range overflows");
+    int rc = cuda(cudaSetDevice(device), "cudaSetDevice");
+    if (rc) return rc;
+    cudaStream_t st = user_stream ? user_stream : stream;
+    std::vector<Job> jobs(1);
+    if ((rc = make_job(p, first, count, 0, jobs[0]))) return rc;
+    std::memcpy(jobs[0].batch_rk, key, 44 * 4);
+    if ((rc = upload_jobs(jobs, st))) return rc;
+    if ((rc = grow(d_out, out_cap, size_t(count) + 1, "failure list"))) return rc;
+    if ((rc = run(jobs, count, st, first, d_out, d_out + count, nullptr, nullptr))) return rc;
+    uint32_t nf = 0;
+    if ((rc = cuda(cudaMemcpyAsync(&nf, d_out + count, 4, cudaMemcpyDeviceToHost, st), "read count")))
+        return rc;
+    if ((rc = cuda(cudaStreamSynchronize(st), "launch sync"))) return rc;
+    if ((rc = check_ctrl())) return rc;
+    if (nf > count) return fail(CMC_ERANGE, "GPU failure count out of range");
+    if (nf && (rc = cuda(cudaMemcpyAsync(out, d_out, size_t(nf) * 4, cudaMemcpyDeviceToHost, st),
+                         "read offsets")))
+        return rc;
+    if (nf && (rc = cuda(cudaStreamSynchronize(st), "offsets sync"))) return rc;
+    *nfailed = nf;
+    return CMC_OK;
+}
+
+int Ctx::launch_device(const cmc_params& p, const uint32_t* d_key_in, uint32_t first,
+                       uint32_t count, uint32_t* d_offsets, uint32_t* d_nfailed, cudaStream_t st) {
+    kernels = 0;
+    if (!d_key_in || !d_offsets || !d_nfailed) return fail(CMC_EINVAL, "null argument");
+    if (!st) st = stream;
+    int rc = cuda(cudaSetDevice(device), "cudaSetDevice");
+    if (rc) return rc;
+    if (count == 0) return cuda(cudaMemsetAsync(d_nfailed, 0, 4, st), "memset count");
+    std::vector<Job> jobs(1);
+    if ((rc = make_job(p, first, count, 0, jobs[0]))) return rc;
+    if ((rc = upload_jobs(jobs, st))) return rc;
+    if ((rc = cuda(cudaMemcpyAsync(d_jobs[0].batch_rk, d_key_in, 44 * 4, cudaMemcpyDeviceToDevice, st),
+                   "copy batch key")))
+        return rc;
+    return run(jobs, count, st, first, d_offsets, d_nfailed, nullptr, nullptr);
+}
+
+}  // namespace cmc
+
+using cmc::Ctx;
+
+extern "C" {
+
+int cmc_init(int device, cmc_ctx** out) {
+    if (!out) return CMC_EINVAL;
+    *out = nullptr;
+    Ctx* c = new (std::nothrow) Ctx();
+    if (!c) return CMC_ENOMEM;
+    const int rc = c->init(device);
+    if (rc) {
+        cmc::g_thread_error = c->err;
+        delete c;
+        return rc;
+    }
+    *out = reinterpret_cast<cmc_ctx*>(c);
+    return CMC_OK;
+}
+
+int cmc_destroy(cmc_ctx* ctx) {
+    delete reinterpret_cast<Ctx*>(ctx);
+    return CMC_OK;
+}
+
+const char* cmc_last_error(const cmc_ctx* ctx) {
+    if (!ctx) return cmc::g_thread_error.c_str();
+    return reinterpret_cast<const Ctx*>(ctx)->err.c_str();
+}
+
+int cmc_launch(cmc_ctx* ctx, const cmc_params* params, const uint32_t batch_key[44],
+               uint32_t first, uint32_t count, uint32_t* out_offsets, uint32_t* out_nfailed) {
+    if (!ctx || !params) return CMC_EINVAL;
+    return reinterpret_cast<Ctx*>(ctx)->launch_host(*params, batch_key, first, count, out_offsets,
+                                                     out_nfailed);
+}
+
+int cmc_launch_device(cmc_ctx* ctx, const cmc_params* params, const uint32_t* d_batch_key,
+                      uint32_t first, uint32_t count, uint32_t* d_out_offsets,
+                      uint32_t* d_out_nfailed, void* stream) {
+    if (!ctx || !params) return CMC_EINVAL;
+    return reinterpret_cast<Ctx*>(ctx)->launch_device(*params, d_batch_key, first, count,
+                                                       d_out_offsets, d_out_nfailed,
+                                                       static_cast<cudaStream_t>(stream));
+}
+
+int cmc_check(cmc_ctx* ctx) {
+    if (!ctx) return CMC_EINVAL;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    int rc = c->cuda(cudaDeviceSynchronize(), "synchronize");
+    if (rc) return rc;
+    return c->check_ctrl();
+}
+
+int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
+    if (!ctx || !name) return CMC_EINVAL;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    const std::string n(name);
+    if (n == "warps_per_group" && value >= 0 && value <= 15) c->force_wg = uint32_t(value);
+    else if (n == "groups" && value >= 0 && value <= cmc::kMaxGroups) c->force_ng = uint32_t(value);
+    else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
+    else if (n == "method" && value >= -1 && value <= 1) c->force_method = int(value);
+    else if (n == "spin_limit" && value >= 0 && value <= 0xffffffffLL)
+        c->spin_limit = value ? uint32_t(value) : (1u << 26);
+    else return c->fail(CMC_EINVAL, "unknown option or value out of range: %s=%lld", name, (long long)value);
+    return CMC_OK;
+}
+
+int cmc_set_stream(cmc_ctx* ctx, void* stream) {
+    if (!ctx) return CMC_EINVAL;
+    reinterpret_cast<Ctx*>(ctx)->user_stream = static_cast<cudaStream_t>(stream);
+    return CMC_OK;
+}
+
+double cmc_last_engine_ms(cmc_ctx* ctx) {
+    if (!ctx) return -1.0;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (c->kernels == 0) return -1.0;
+    float ms = 0.f;
+    if (cudaEventSynchronize(c->ev_stop) != cudaSuccess) return -1.0;
+    if (cudaEventElapsedTime(&ms, c->ev_start, c->ev_stop) != cudaSuccess) return -1.0;
+    return ms;
+}
+
+uint32_t cmc_last_kernel_count(const cmc_ctx* ctx) {
+    return ctx ? reinterpret_cast<const Ctx*>(ctx)->kernels : 0;
+}
+
+const char* cmc_last_plan(const cmc_ctx* ctx) {
+    return ctx ? reinterpret_cast<const Ctx*>(ctx)->plan_text.c_str() : "";
+}
+
+}  // extern "C"

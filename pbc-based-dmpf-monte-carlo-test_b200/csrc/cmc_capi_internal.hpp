@@ -1,0 +1,68 @@
+// cmc_capi_internal.hpp -- the context behind the opaque cmc_ctx handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "cmc.h"
+#include "cmc_engine.cuh"
+
+namespace cmc {
+
+struct Plan {
+    uint32_t ng = 0, wg = 0, ns = 0;
+    bool slots_smem = true;
+    uint32_t slot_stride = 0, bins_bytes = 0, group_bytes = 0;
+    uint32_t group_off = 0, slots_off = 0, smem_bytes = 0, threads = 0, ctas = 0;
+    int variant = 0;  // 0: u16 map/bins, 1: u32 map/bins, 2: u32 + 64-bit PRP domain
+};
+
+struct Ctx {
+    int device = -1;
+    int sms = 0;
+    size_t smem_optin = 0;
+    cudaStream_t stream = nullptr;       // the context's own stream
+    cudaStream_t user_stream = nullptr;  // cmc_set_stream override
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    uint32_t* d_t0 = nullptr;  // T0 table, FIPS KAT schedule, self-test output
+    Ctrl* d_ctrl = nullptr;
+    Job* d_jobs = nullptr;
+    size_t jobs_cap = 0;
+    uint32_t* d_bits = nullptr;
+    size_t bits_cap = 0;
+    uint32_t* d_out = nullptr;
+    size_t out_cap = 0;
+    char* d_slots = nullptr;
+    size_t slots_cap = 0;
+    uint32_t* d_key = nullptr;
+    std::string err, plan_text;
+    uint32_t kernels = 0;
+    Plan last_plan;
+    unsigned long long last_walks = 0, last_probes = 0;
+    // tuning overrides (0 = automatic)
+    uint32_t force_wg = 0, force_ng = 0, force_global_slots = 0;
+    int force_method = -1;  // -1 auto, 0 direct, 1 cache
+    uint32_t spin_limit = 1u << 26;
+
+    ~Ctx();
+    int init(int dev);
+    int fail(int code, const char* fmt, ...);
+    int cuda(cudaError_t e, const char* what);
+    template <typename T>
+    int grow(T*& ptr, size_t& cap, size_t need, const char* what);
+    int make_job(const cmc_params& p, uint32_t first, uint32_t count, uint64_t base, Job& j);
+    int plan(const std::vector<Job>& jobs, Plan& pl);
+    int upload_jobs(const std::vector<Job>& jobs, cudaStream_t st);
+    int run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint32_t value_base,
+            uint32_t* d_out, uint32_t* d_count, unsigned long long* job_failed,
+            unsigned long long* job_done);
+    int check_ctrl();
+    int launch_host(const cmc_params& p, const uint32_t key[44], uint32_t first, uint32_t count,
+                    uint32_t* out, uint32_t* nfailed);
+    int launch_device(const cmc_params& p, const uint32_t* d_key, uint32_t first, uint32_t count,
+                      uint32_t* d_offsets, uint32_t* d_nfailed, cudaStream_t st);
+};
+
+}  // namespace cmc

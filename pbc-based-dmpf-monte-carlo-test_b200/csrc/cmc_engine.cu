@@ -1,0 +1,640 @@
+// cmc_engine.cu -- the per-trial Monte Carlo path on sm_100a.
+//
+// One persistent CTA per SM.  Its warps are split into
+//   * NG producer groups of WG warps.  A group takes one trial at a time from
+//     a global work counter, derives the trial's PRP key and walk seed
+//     (cuckoo_bench.cu:226-238), and evaluates the bucket of every (item,
+//     copy) pair -- the map -- either by direct 8-round AES Feistel passes or
+//     from an 8*2^h round cache it builds in shared memory first
+//     (gpu_shared.cuh:70-91 is the reference's warp-per-trial version).  The
+//     map and an empty table go into a slot.
+//   * one walker warp.  Lane s owns slot s and runs the serial cuckoo
+//     insertion walk (cuckoo_core.hpp:117-161) of the trial in it while the
+//     producers already build later maps.  The reference runs that walk on
+//     lane 0 of the producing warp with 31 lanes idle (gpu_shared.cuh:93).
+// Failures are set in a bitmap indexed by the launch's global trial index and
+// compacted in order by cmc_compact_failures (the reference appends offsets
+// through an atomic counter and sorts on the host, cuckoo_bench.cu:313-316,738).
+//
+// All waits (slot hand-off, end of work) are bounded: after spin_limit polls
+// the kernel records CMC_ETIMEOUT in Ctrl and returns.
+#include <cstdint>
+
+#include "cmc_aes.cuh"
+#include "cmc_engine.cuh"
+
+namespace cmc {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kErrTimeout = 4;  // == -CMC_ETIMEOUT
+constexpr uint32_t kErrRange = 5;    // == -CMC_ERANGE
+
+struct GroupHeader {
+    unsigned long long gidx;
+    uint32_t job, offset;
+    uint32_t rk[44];
+    uint32_t r1[8][8];  // Round1 {c0, c1, c2, c3, w3hi} per Feistel round (padded)
+    unsigned long long walk, rnd, shift, step;
+    uint32_t slot, cand_next, abort, pad;
+};
+
+struct SlotHeader {
+    unsigned long long gidx, walk, rnd;
+    uint32_t job, offset;
+};
+
+struct CtaShared {
+    uint32_t slot_state[kMaxSlots];
+    SlotHeader slot_hdr[kMaxSlots];
+    uint32_t groups_done;
+};
+
+constexpr uint32_t kCtaSharedOff = kTableBytes;
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];"
+                 : "=r"(v)
+                 : "r"((uint32_t)__cvta_generic_to_shared(p))
+                 : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(p)),
+                 "r"(v)
+                 : "memory");
+}
+
+__device__ __forceinline__ void group_sync(uint32_t g, uint32_t nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ uint64_t splitmix(uint64_t& s) {
+    s += 0x9E3779B97F4A7C15ULL;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// floor(y / width) for y < 2^32 with magic = floor((2^32 - 1) / width):
+// the estimate is at most two below the quotient and never above it.
+__device__ __forceinline__ uint32_t div_width(uint32_t y, uint32_t width, uint32_t magic) {
+    uint32_t q = __umulhi(y, magic);
+    uint32_t r = y - q * width;
+    if (r >= width) { ++q; r -= width; }
+    if (r >= width) { ++q; }
+    return q;
+}
+
+__device__ __forceinline__ uint32_t find_job(const Job* jobs, uint32_t njobs, uint64_t g) {
+    uint32_t lo = 0, hi = njobs;  // last job with trial_base <= g
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (jobs[mid].trial_base <= g) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Warp-aggregated claim of candidate indices from a shared counter.
+__device__ __forceinline__ uint32_t claim(uint32_t* counter, bool need, uint32_t lane) {
+    const unsigned m = __ballot_sync(kFull, need);
+    uint32_t base = 0;
+    const int leader = __ffs(m) - 1;
+    if (m && (int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+    base = __shfl_sync(kFull, base, leader < 0 ? 0 : leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+template <typename MapT, typename BinT>
+struct SlotView {
+    BinT* bins;
+    MapT* map;
+};
+
+// ---------------------------------------------------------------- producer --
+
+template <typename MapT, bool WIDE>
+__device__ __forceinline__ void build_map_direct(const Lanes& L, const Job& J, GroupHeader* gh,
+                                                 const PrpKey& key, MapT* map, uint32_t lane) {
+    const uint32_t k = J.k, ncand = J.pnum * k, h = J.half_bits;
+    const uint64_t mask = J.mask, domain = J.domain;
+    const bool sequential = J.input_mode == 0;
+    const uint64_t shift = gh->shift, step = gh->step, range_mask = J.range_mask;
+    uint32_t c = claim(&gh->cand_next, true, lane);
+    bool has = c < ncand;
+    uint64_t left = 0, right = 0;
+    auto start = [&](uint32_t cand) {
+        const uint32_t o = cand / k, j = cand - o * k;
+        const uint64_t e = sequential ? (uint64_t)o : (shift + (uint64_t)o * step) & range_mask;
+        const uint64_t y = e * k + j;
+        left = y >> h;
+        right = y & mask;
+    };
+    if (has) start(c);
+    while (__any_sync(kFull, has)) {
+        if constexpr (!WIDE) {
+            uint32_t l = (uint32_t)left, r = (uint32_t)right;
+#pragma unroll 1
+            for (uint32_t rr = 0; rr < 8; ++rr) {
+                const uint4 c4 = *reinterpret_cast<const uint4*>(&gh->r1[rr][0]);
+                const Round1 rc{c4.x, c4.y, c4.z, c4.w, gh->r1[rr][4]};
+                const uint32_t f = prp_f(L, key, rc, r) & (uint32_t)mask;
+                const uint32_t nr = (l ^ f) & (uint32_t)mask;
+                l = r;
+                r = nr;
+            }
+            left = l;
+            right = r;
+        } else {
+#pragma unroll 1
+            for (uint32_t rr = 0; rr < 8; ++rr) {
+                const uint32_t f = prp_f_wide(L, gh->rk, rr, h, (uint32_t)right);
+                const uint64_t nr = (left ^ ((uint64_t)f & mask)) & mask;
+                left = right;
+                right = nr;
+            }
+        }
+        const uint64_t y = (left << h) | right;
+        const bool done = has && y < domain;
+        if (done) {
+            uint32_t b;
+            if constexpr (!WIDE) b = div_width((uint32_t)y, (uint32_t)J.width, J.width_magic);
+            else b = (uint32_t)(y / J.width);
+            map[c] = (MapT)b;
+        } else if (has) {
+            left = y >> h;
+            right = y & mask;
+        }
+        const uint32_t nc = claim(&gh->cand_next, done, lane);
+        if (done) {
+            c = nc;
+            has = c < ncand;
+            if (has) start(c);
+        }
+    }
+}
+
+template <typename MapT>
+__device__ __forceinline__ void build_map_cache(const Job& J, GroupHeader* gh,
+                                                const uint16_t* cache, MapT* map,
+                                                uint32_t lane) {
+    const uint32_t k = J.k, ncand = J.pnum * k, h = J.half_bits;
+    const uint32_t mask = (uint32_t)J.mask;
+    const uint32_t domain_m1 = (uint32_t)(J.domain - 1);
+    const bool sequential = J.input_mode == 0;
+    const uint64_t shift = gh->shift, step = gh->step, range_mask = J.range_mask;
+    uint32_t c = claim(&gh->cand_next, true, lane);
+    bool has = c < ncand;
+    uint32_t l = 0, r = 0;
+    auto start = [&](uint32_t cand) {
+        const uint32_t o = cand / k, j = cand - o * k;
+        const uint64_t e = sequential ? (uint64_t)o : (shift + (uint64_t)o * step) & range_mask;
+        const uint32_t y = (uint32_t)(e * k + j);
+        l = y >> h;
+        r = y & mask;
+    };
+    if (has) start(c);
+    while (__any_sync(kFull, has)) {
+#pragma unroll
+        for (uint32_t rr = 0; rr < 8; ++rr) {
+            const uint32_t f = cache[(rr << h) | r];
+            const uint32_t nr = l ^ f;
+            l = r;
+            r = nr;
+        }
+        const uint32_t y = (l << h) | r;
+        const bool done = has && y <= domain_m1;
+        if (done) {
+            map[c] = (MapT)div_width(y, (uint32_t)J.width, J.width_magic);
+        } else if (has) {
+            l = y >> h;
+            r = y & mask;
+        }
+        const uint32_t nc = claim(&gh->cand_next, done, lane);
+        if (done) {
+            c = nc;
+            has = c < ncand;
+            if (has) start(c);
+        }
+    }
+}
+
+template <typename MapT, typename BinT, bool WIDE>
+__device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaShared* cs, uint32_t g) {
+    const uint32_t gthreads = a.wg * 32;
+    const uint32_t gt = threadIdx.x - g * gthreads;
+    const uint32_t lane = threadIdx.x & 31;
+    const Lanes L{lane * 4, lane * 4 + 128};
+    char* gbase = smem + a.group_off + g * a.group_bytes;
+    GroupHeader* gh = reinterpret_cast<GroupHeader*>(gbase);
+    uint16_t* cache = reinterpret_cast<uint16_t*>(gbase + sizeof(GroupHeader));
+    const uint32_t slots_per_group = a.ns / a.ng;
+    uint32_t cursor = 0;
+
+    for (;;) {
+        if (gt == 0) {
+            const unsigned long long gi = atomicAdd(&a.ctrl->next, 1ULL);
+            gh->gidx = gi;
+            gh->abort = 0;
+            if (gi < a.total) {
+                const uint32_t j = find_job(a.jobs, a.njobs, gi);
+                gh->job = j;
+                gh->offset = a.jobs[j].first + (uint32_t)(gi - a.jobs[j].trial_base);
+            }
+        }
+        group_sync(g, gthreads);
+        const unsigned long long gi = gh->gidx;
+        if (gi >= a.total) break;
+        const Job& J = a.jobs[gh->job];
+
+        // Per-trial PRP key and walk seed (cuckoo_bench.cu:226-238).
+        if (gt == 0) {
+            uint32_t w[4];
+            encrypt_full(L, J.batch_rk, 0x4b455931u, 0, gh->offset, 0x50525031u, w);
+            expand_key(L, w[0], w[1], w[2], w[3], gh->rk);
+            encrypt_full(L, J.batch_rk, 0x57414c4bu, 0, gh->offset, 0x524e4731u, w);
+            uint64_t walk = ((uint64_t)w[0] << 32) | w[1];
+            const uint64_t shift = (((uint64_t)w[2] << 32) | w[3]) & J.range_mask;
+            uint64_t input_state = shift ^ 0xd1b54a32d192ed03ULL;
+            gh->step = (splitmix(input_state) | 1ULL) & J.range_mask;
+            gh->shift = shift;
+            gh->rnd = splitmix(walk);
+            gh->walk = walk;
+            gh->cand_next = 0;
+            // Next slot of this group; wait until its previous walk is done.
+            const uint32_t slot = g + a.ng * (cursor % slots_per_group);
+            uint32_t spins = 0;
+            while (ld_acquire(&cs->slot_state[slot]) != kSlotFree) {
+                __nanosleep(256);
+                if (++spins > a.spin_limit) {
+                    atomicExch(&a.ctrl->error, kErrTimeout);
+                    atomicExch(&a.ctrl->where, 1u);
+                    gh->abort = 1;
+                    break;
+                }
+            }
+            gh->slot = slot;
+        }
+        ++cursor;
+        group_sync(g, gthreads);
+        if (gh->abort) break;
+        if constexpr (!WIDE) {
+            if (gt < 8) {
+                const Round1 c = round1_consts(L, gh->rk, gt, J.half_bits);
+                gh->r1[gt][0] = c.c0; gh->r1[gt][1] = c.c1; gh->r1[gt][2] = c.c2;
+                gh->r1[gt][3] = c.c3; gh->r1[gt][4] = c.w3hi;
+            }
+        }
+        group_sync(g, gthreads);
+
+        const uint32_t slot = gh->slot;
+        char* sbase = a.gslots ? a.gslots + ((size_t)blockIdx.x * a.ns + slot) * a.slot_stride
+                               : smem + a.slots_off + (size_t)slot * a.slot_stride;
+        BinT* bins = reinterpret_cast<BinT*>(sbase);
+        MapT* map = reinterpret_cast<MapT*>(sbase + a.bins_bytes);
+        {
+            const uint32_t nvec = (J.buckets * (uint32_t)sizeof(BinT) + 15) / 16;
+            uint4* b4 = reinterpret_cast<uint4*>(bins);
+            for (uint32_t i = gt; i < nvec; i += gthreads) b4[i] = make_uint4(kFull, kFull, kFull, kFull);
+        }
+        PrpKey key;
+        if constexpr (!WIDE) prp_key_from_schedule(gh->rk, key);
+        if (!WIDE && J.method == kMethodCache) {
+            const uint32_t h = J.half_bits, entries = 8u << h, m = (uint32_t)J.mask;
+            for (uint32_t e = gt; e < entries; e += gthreads) {
+                const uint32_t rr = e >> h;
+                const uint4 c4 = *reinterpret_cast<const uint4*>(&gh->r1[rr][0]);
+                const Round1 rc{c4.x, c4.y, c4.z, c4.w, gh->r1[rr][4]};
+                cache[e] = (uint16_t)(prp_f(L, key, rc, e & m) & m);
+            }
+            group_sync(g, gthreads);
+            build_map_cache<MapT>(J, gh, cache, map, lane);
+        } else {
+            build_map_direct<MapT, WIDE>(L, J, gh, key, map, lane);
+        }
+        __threadfence_block();
+        group_sync(g, gthreads);
+        if (gt == 0) {
+            SlotHeader& sh = cs->slot_hdr[slot];
+            sh.gidx = gi;
+            sh.walk = gh->walk;
+            sh.rnd = gh->rnd;
+            sh.job = gh->job;
+            sh.offset = gh->offset;
+            st_release(&cs->slot_state[slot], kSlotReady);
+        }
+    }
+    if (gt == 0) {
+        __threadfence_block();
+        atomicAdd(&cs->groups_done, 1u);
+    }
+}
+
+// ------------------------------------------------------------------ walker --
+
+template <typename MapT, typename BinT>
+struct Walk {
+    static constexpr uint32_t kShift = sizeof(BinT) == 2 ? 14 : 16;
+    static constexpr uint32_t kOrdMask = (1u << kShift) - 1u;
+    static constexpr BinT kEmpty = (BinT)~(BinT)0;
+
+    const MapT* map;
+    BinT* bins;
+    uint64_t walk, rnd, magic;
+    uint32_t magic_shift, k, t, kick, bgh, nbins;
+    uint32_t item, cur, count, phase, choice, target;
+    bool active, failed, bad;
+
+    __device__ __forceinline__ void begin(const Job& J, const SlotHeader& h, BinT* b, const MapT* m) {
+        map = m;
+        bins = b;
+        walk = h.walk;
+        rnd = h.rnd;
+        k = J.k;
+        t = J.pnum;
+        kick = J.kick;
+        nbins = J.buckets;
+        bgh = J.mode == 1;
+        // randomness / k as umulhi(rnd, magic) >> magic_shift for k in {2,3,4}
+        magic = k == 3 ? 0xAAAAAAAAAAAAAAABULL : (k == 2 ? 0x8000000000000000ULL : 0x4000000000000000ULL);
+        magic_shift = k == 3 ? 1 : 0;
+        item = 0; cur = 0; count = 0; phase = 0; choice = 0; target = 0;
+        active = true;
+        failed = false;
+        bad = false;
+    }
+
+    // A map entry is a bucket index < B by construction (y < D = B * width);
+    // anything else is recorded as an error instead of being dereferenced.
+    __device__ __forceinline__ bool out_of_range(uint32_t b) {
+        if (b < nbins) return false;
+        bad = true;
+        failed = true;
+        active = false;
+        return true;
+    }
+
+    __device__ __forceinline__ BinT pack(uint32_t o, uint32_t j) const { return (BinT)(o | (j << kShift)); }
+
+    // One probe of the walk.  BGH25: cuckoo_core.hpp:123-133; DRRT18: :134-158.
+    __device__ __forceinline__ void step() {
+        if (bgh) {
+            if (rnd < k) rnd = splitmix(walk);
+            const uint64_t q = __umul64hi(rnd, magic) >> magic_shift;
+            const uint32_t which = (uint32_t)(rnd - q * k);
+            rnd = q;
+            const uint32_t tgt = map[cur * k + which];
+            if (out_of_range(tgt)) return;
+            const BinT old = bins[tgt];
+            if (old == kEmpty) {
+                bins[tgt] = pack(cur, which);
+                cur = ++item;
+                count = 0;
+                if (item == t) active = false;
+            } else if (++count > kick) {
+                failed = true;
+                active = false;
+            } else {
+                bins[tgt] = pack(cur, which);
+                cur = old & kOrdMask;
+            }
+        } else if (phase == 0) {
+            // a new item tries its copies in order
+            const uint32_t b = map[item * k + choice];
+            if (out_of_range(b)) return;
+            if (bins[b] == kEmpty) {
+                bins[b] = pack(item, choice);
+                ++item;
+                choice = 0;
+                if (item == t) active = false;
+            } else if (++choice == k) {
+                phase = 1;
+                cur = item;
+                choice = 0;
+                target = map[item * k];
+                count = 0;
+                if (out_of_range(target)) return;
+            }
+        } else {
+            const BinT displaced = bins[target];
+            if (displaced == kEmpty) {
+                bins[target] = pack(cur, choice);
+                ++item;
+                phase = 0;
+                choice = 0;
+                if (item == t) active = false;
+                return;
+            }
+            if (count >= kick) {
+                failed = true;
+                active = false;
+                return;
+            }
+            bins[target] = pack(cur, choice);
+            cur = displaced & kOrdMask;
+            choice = (displaced >> kShift) & 3u;
+            const uint32_t previous = target;
+            bool found = false;
+            for (uint32_t s = 0; s < k; ++s) {
+                choice = choice + 1 == k ? 0 : choice + 1;
+                const uint32_t next = map[cur * k + choice];
+                if (next != previous) { target = next; found = true; break; }
+            }
+            if (found && out_of_range(target)) return;
+            if (!found) {
+                failed = true;
+                active = false;
+                return;
+            }
+            ++count;
+        }
+    }
+};
+
+template <typename MapT, typename BinT>
+__device__ __forceinline__ void walker(const EngineArgs& a, char* smem, CtaShared* cs) {
+    const uint32_t lane = threadIdx.x & 31;
+    Walk<MapT, BinT> w;
+    w.active = false;
+    bool busy = false;  // holds a slot
+    unsigned long long gidx = 0;
+    uint32_t job = 0;
+    unsigned long long probes = 0, walks = 0;
+    uint32_t idle = 0;
+    for (;;) {
+        if (!busy && lane < a.ns && ld_acquire(&cs->slot_state[lane]) == kSlotReady) {
+            const SlotHeader h = cs->slot_hdr[lane];
+            char* sbase = a.gslots ? a.gslots + ((size_t)blockIdx.x * a.ns + lane) * a.slot_stride
+                                   : smem + a.slots_off + (size_t)lane * a.slot_stride;
+            job = h.job;
+            gidx = h.gidx;
+            w.begin(a.jobs[job], h, reinterpret_cast<BinT*>(sbase),
+                    reinterpret_cast<const MapT*>(sbase + a.bins_bytes));
+            busy = true;
+        }
+#pragma unroll 1
+        for (int s = 0; s < 64 && w.active; ++s) {
+            w.step();
+            ++probes;
+        }
+        if (busy && !w.active) {
+            if (w.bad) {
+                atomicExch(&a.ctrl->error, kErrRange);
+                atomicExch(&a.ctrl->where, 3u);
+            }
+            if (w.failed) {
+                atomicOr(&a.fail_bits[gidx >> 5], 1u << (gidx & 31));
+                if (a.job_failed) atomicAdd(&a.job_failed[job], 1ULL);
+            }
+            if (a.job_done) atomicAdd(&a.job_done[job], 1ULL);
+            ++walks;
+            busy = false;
+            st_release(&cs->slot_state[lane], kSlotFree);
+        }
+        if (!__any_sync(kFull, busy)) {
+            // Every lane acquires groups_done itself; the warp leaves only when
+            // all lanes saw every group finished and no slot is still READY.
+            const bool done = __all_sync(kFull, ld_acquire(&cs->groups_done) == a.ng);
+            const bool ready = lane < a.ns && ld_acquire(&cs->slot_state[lane]) == kSlotReady;
+            if (!__any_sync(kFull, ready)) {
+                if (done) break;
+                __nanosleep(128);
+                if (++idle > a.spin_limit) {
+                    if (lane == 0) {
+                        atomicExch(&a.ctrl->error, kErrTimeout);
+                        atomicExch(&a.ctrl->where, 2u);
+                    }
+                    break;
+                }
+            }
+        } else {
+            idle = 0;
+        }
+    }
+    // warp totals for diagnostics
+    for (int o = 16; o; o >>= 1) {
+        probes += __shfl_xor_sync(kFull, probes, o);
+        walks += __shfl_xor_sync(kFull, walks, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&a.ctrl->probes, probes);
+        atomicAdd(&a.ctrl->walks, walks);
+    }
+}
+
+}  // namespace
+
+template <typename MapT, typename BinT, bool WIDE>
+__global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
+    char* smem = cmc_dyn_smem;
+    // Bank-replicated table: row x = [T0[x] x 32][ror16(T0[x]) x 32].
+    {
+        uint32_t* tw = reinterpret_cast<uint32_t*>(smem);
+        for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) {
+            const uint32_t v = __ldg(&a.t0[i >> 6]);
+            tw[i] = (i & 32) ? __funnelshift_r(v, v, 16) : v;
+        }
+    }
+    CtaShared* cs = reinterpret_cast<CtaShared*>(smem + kCtaSharedOff);
+    if (threadIdx.x < kMaxSlots) cs->slot_state[threadIdx.x] = kSlotFree;
+    if (threadIdx.x == 0) cs->groups_done = 0;
+    __syncthreads();
+    const uint32_t warp = threadIdx.x >> 5;
+    if (warp < a.ng * a.wg) producer<MapT, BinT, WIDE>(a, smem, cs, warp / a.wg);
+    else if (warp == a.ng * a.wg) walker<MapT, BinT>(a, smem, cs);
+}
+
+// Ordered failure list from the bitmap: one CTA, block-wide exclusive scan.
+// out[i] = value_base + (index of the i-th set bit); *count = number of bits.
+__global__ void __launch_bounds__(1024) cmc_compact_failures(const uint32_t* __restrict__ bits,
+                                                             uint64_t nbits, uint32_t value_base,
+                                                             uint32_t* __restrict__ out,
+                                                             uint32_t* __restrict__ count) {
+    __shared__ uint32_t warp_sums[32];
+    const uint64_t words = (nbits + 31) / 32;
+    const uint64_t per = (words + blockDim.x - 1) / blockDim.x;
+    const uint64_t w0 = per * threadIdx.x, w1 = min(words, w0 + per);
+    uint32_t mine = 0;
+    for (uint64_t w = w0; w < w1; ++w) mine += __popc(bits[w]);
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t nw = blockDim.x / 32;
+        uint32_t v = lane < nw ? warp_sums[lane] : 0, s = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(kFull, s, o);
+            if (lane >= (uint32_t)o) s += u;
+        }
+        if (lane < nw) warp_sums[lane] = s - v;  // exclusive
+        if (lane == nw - 1) *count = s;
+    }
+    __syncthreads();
+    uint32_t at = warp_sums[warp] + incl - mine;
+    for (uint64_t w = w0; w < w1; ++w) {
+        uint32_t b = bits[w];
+        while (b) {
+            const int i = __ffs(b) - 1;
+            b &= b - 1;
+            out[at++] = value_base + (uint32_t)(w * 32 + i);
+        }
+    }
+}
+
+// Device self-test: the FIPS-197 AES-128 vector on every lane through the
+// shared-memory table, and the 124-lookup PRP round function against the
+// full encryption for pseudo-random keys, rounds and inputs.
+__global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out) {
+    char* smem = cmc_dyn_smem;
+    uint32_t* tw = reinterpret_cast<uint32_t*>(smem);
+    for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) {
+        const uint32_t v = t0[i >> 6];
+        tw[i] = (i & 32) ? __funnelshift_r(v, v, 16) : v;
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    const Lanes L{lane * 4, lane * 4 + 128};
+    uint32_t c[4];
+    encrypt_full(L, fips_rk, 0x00112233u, 0x44556677u, 0x8899aabbu, 0xccddeeffu, c);
+    uint32_t bad = 0;
+    if (c[0] != 0x69c4e0d8u || c[1] != 0x6a7b0430u || c[2] != 0xd8cdb780u || c[3] != 0x70b4c55au)
+        bad |= 1;
+    // key expansion from words reproduces the FIPS schedule
+    uint32_t rk[44];
+    expand_key(L, fips_rk[0], fips_rk[1], fips_rk[2], fips_rk[3], rk);
+    for (int i = 0; i < 44; ++i)
+        if (rk[i] != fips_rk[i]) bad |= 2;
+    uint64_t s = 0x1234567ULL + threadIdx.x;
+    for (int it = 0; it < 8; ++it) {
+        const uint32_t a = (uint32_t)splitmix(s), b = (uint32_t)splitmix(s);
+        const uint32_t cc = (uint32_t)splitmix(s), d = (uint32_t)splitmix(s);
+        expand_key(L, a, b, cc, d, rk);
+        PrpKey key;
+        prp_key_from_schedule(rk, key);
+        const uint32_t h = 2 + (uint32_t)(splitmix(s) % 15);  // 2..16
+        const uint32_t r = (uint32_t)(splitmix(s) & 7);
+        const uint32_t R = (uint32_t)splitmix(s) & ((1u << h) - 1u);
+        const Round1 rc = round1_consts(L, rk, r, h);
+        uint32_t full[4];
+        encrypt_full(L, rk, 0x43455350u, r, h, R, full);
+        if ((prp_f(L, key, rc, R) & 0xffffu) != (full[3] & 0xffffu)) bad |= 4;
+    }
+    out[threadIdx.x] = bad;
+}
+
+// Explicit instantiations used by the launcher.
+template __global__ void cmc_engine<uint16_t, uint16_t, false>(const EngineArgs);
+template __global__ void cmc_engine<uint32_t, uint32_t, false>(const EngineArgs);
+template __global__ void cmc_engine<uint32_t, uint32_t, true>(const EngineArgs);
+
+}  // namespace cmc

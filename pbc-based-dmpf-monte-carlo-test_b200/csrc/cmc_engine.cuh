@@ -1,0 +1,60 @@
+// cmc_engine.cuh -- device data structures shared by the engine kernels and
+// the host planner.
+#pragma once
+#include <cstdint>
+
+namespace cmc {
+
+constexpr uint32_t kMethodDirect = 0;  // candidates by 8-round AES Feistel passes
+constexpr uint32_t kMethodCache = 1;   // 8*2^h round cache in shared memory, then lookups
+
+constexpr uint32_t kSlotFree = 0;
+constexpr uint32_t kSlotReady = 1;
+
+constexpr uint32_t kMaxSlots = 32;  // one walker lane per slot
+constexpr uint32_t kEngineTableBytes = 65536;  // replicated T-table at shared offset 0
+constexpr uint32_t kMaxGroups = 14; // named barriers 1..14
+
+// One experiment configuration applied to a contiguous run of trials of one
+// batch.  A launch processes trials [0, total) of the concatenation of its
+// jobs; job j owns global indices [trial_base, trial_base + count).
+struct Job {
+    uint32_t batch_rk[44];  // batch key schedule (plain words)
+    uint32_t pnum, k, buckets, kick;
+    uint32_t mode, input_mode, half_bits, method;
+    uint64_t domain, mask, range_mask, width;
+    uint32_t width_magic;   // floor((2^32 - 1) / width) when domain < 2^32
+    uint32_t first;         // first within-batch offset
+    uint32_t count;         // trials of this job in the launch
+    uint32_t user;          // caller tag (job id in batched/served mode)
+    uint64_t trial_base;
+};
+
+struct Ctrl {
+    unsigned long long next;   // work counter: next global trial index
+    unsigned int error;        // 0, or a CMC_E* code (positive here)
+    unsigned int where;        // which wait gave up (diagnostics)
+    unsigned long long walks;  // walks completed (all jobs)
+    unsigned long long probes; // probes spent (all jobs)
+};
+
+struct EngineArgs {
+    const Job* jobs;
+    uint32_t njobs;
+    uint64_t total;
+    Ctrl* ctrl;
+    uint32_t* fail_bits;                // bit g = global trial g failed
+    unsigned long long* job_failed;     // per job (optional)
+    unsigned long long* job_done;       // per job (optional)
+    char* gslots;                       // global slot pool (nullptr: slots in smem)
+    const uint32_t* t0;                 // 256-word T0 table in global memory
+    uint32_t slot_stride;               // bytes per slot
+    uint32_t bins_bytes;                // map starts this far into a slot
+    uint32_t ng, wg, ns;                // groups, warps per group, slots
+    uint32_t group_bytes;               // per-group smem (header + cache)
+    uint32_t group_off;                 // smem offset of group 0
+    uint32_t slots_off;                 // smem offset of slot 0 (smem slots)
+    uint32_t spin_limit;                // bounded waits (polls of ~0.5 us)
+};
+
+}  // namespace cmc
