@@ -176,12 +176,19 @@ def cpu_run(n_trials: int, batch: int, threads: int):
     return time.perf_counter() - t0, kind, n
 
 
+def cpu_sample_size(threads: int, target_seconds: float) -> tuple[int, float, str]:
+    """Grow the sample until one run takes about target_seconds (cap 2^20)."""
+    n = max(256, threads * 16)
+    while True:
+        secs, kind, _ = cpu_run(n, 0, threads)
+        if secs >= target_seconds * 0.5 or n >= 1 << 20:
+            return n, secs, kind
+        n = int(min(1 << 20, max(2 * n, n * target_seconds / max(secs, 1e-3))))
+
+
 def cpu_baseline(target_seconds: float = 10.0) -> dict:
     threads = host_threads()
-    secs, kind, _ = cpu_run(max(64, threads * 8), 0, threads)
-    rate = max(64, threads * 8) / max(secs, 1e-6)
-    n = int(min(1 << 20, max(256, rate * target_seconds)))
-    secs, kind, _ = cpu_run(n, 0, threads)
+    n, secs, kind = cpu_sample_size(threads, target_seconds)
     return {"value": n / secs, "unit": "trials/s", "cores": threads, "kind": kind,
             "sample": f"first {n} trials of batch 0 of the bench workload "
                       f"({'reference cpu_batch_launch, AES-NI' if kind == 'reference' else 'oracle port'}, "
@@ -193,9 +200,8 @@ def run_reference_arm(args, rank: int, world: int) -> None:
         return
     threads = host_threads()
     w = WORKLOAD
-    # bounded sample per step, sized from a short probe (~1 s per step)
-    secs, kind, _ = cpu_run(max(64, threads * 8), 0, threads)
-    per_step = int(min(1 << 20, max(128, (max(64, threads * 8) / max(secs, 1e-6)) * 1.0)))
+    # bounded sample per step: about 2 s of CPU work each
+    per_step, _, kind = cpu_sample_size(threads, 2.0)
     for s in range(args.warmup):
         cpu_run(per_step, s, threads)
     total = 0.0
@@ -251,7 +257,10 @@ def main():
     p = cmc.parameters(w["mode"], w["pnum"], w["ell_i"], w["k"], w["buckets"], w["kick"],
                        w["input_mode"])
     n = 1 << w["bt"]
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the legacy default stream's handle is NULL, which the
+    # C ABI reads as "the context's own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     d_out = torch.empty(n, dtype=torch.int32, device="cuda")
     d_n = torch.zeros(1, dtype=torch.int32, device="cuda")
