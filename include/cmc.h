@@ -107,6 +107,12 @@ int cmc_set_stream(cmc_ctx* ctx, void* stream);
  * launch), in milliseconds; waits for it to finish.  -1 on error. */
 double cmc_last_engine_ms(cmc_ctx* ctx);
 
+/* Counters of the last checked launch (cmc_launch, or cmc_check after
+ * cmc_launch_device): out[0] walks, out[1] probes, out[2] cycles producer
+ * groups waited for a free slot, out[3] cycles walker warps had nothing to
+ * walk, out[4] walker warps' total cycles, out[5] device error code. */
+int cmc_last_stats(cmc_ctx* ctx, uint64_t out[6]);
+
 /* Kernels launched by the last cmc_launch* call on this context. */
 uint32_t cmc_last_kernel_count(const cmc_ctx* ctx);
 /* Human-readable description of the last launch plan (engine, groups, ...). */

@@ -36,7 +36,7 @@ EXPORTS = (
     "cmc_derive_params", "cmc_batch_key", "cmc_host_aes128", "cmc_init", "cmc_destroy",
     "cmc_last_error", "cmc_launch", "cmc_launch_device", "cmc_check",
     "cmc_last_kernel_count", "cmc_last_plan", "cmc_set_option",
-    "cmc_set_stream", "cmc_last_engine_ms",
+    "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats",
 )
 
 
@@ -108,6 +108,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.cmc_set_stream.restype = ctypes.c_int
     lib.cmc_last_engine_ms.argtypes = [vp]
     lib.cmc_last_engine_ms.restype = ctypes.c_double
+    lib.cmc_last_stats.argtypes = [vp, P(u64)]
+    lib.cmc_last_stats.restype = ctypes.c_int
     lib.cmc_last_plan.argtypes = [vp]
     lib.cmc_last_plan.restype = ctypes.c_char_p
     if path is None:
@@ -209,6 +211,12 @@ class Context:
 
     def last_engine_ms(self) -> float:
         return self.lib.cmc_last_engine_ms(self.handle)
+
+    def last_stats(self) -> dict:
+        out = (ctypes.c_uint64 * 6)()
+        self.lib.cmc_last_stats(self.handle, out)
+        keys = ("walks", "probes", "slot_wait_cycles", "walker_idle_cycles", "walker_cycles", "error")
+        return dict(zip(keys, list(out)))
 
     @property
     def last_plan(self) -> str:

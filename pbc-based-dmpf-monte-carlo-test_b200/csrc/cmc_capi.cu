@@ -235,8 +235,7 @@ int Ctx::check_ctrl() {
     Ctrl c{};
     int rc = cuda(cudaMemcpy(&c, d_ctrl, sizeof c, cudaMemcpyDeviceToHost), "read ctrl");
     if (rc) return rc;
-    last_walks = c.walks;
-    last_probes = c.probes;
+    last_ctrl = c;
     if (c.error)
         return fail(-int(c.error), "device wait gave up (site %u): results discarded", c.where);
     return CMC_OK;
@@ -436,6 +435,19 @@ double cmc_last_engine_ms(cmc_ctx* ctx) {
     if (cudaEventSynchronize(c->ev_stop) != cudaSuccess) return -1.0;
     if (cudaEventElapsedTime(&ms, c->ev_start, c->ev_stop) != cudaSuccess) return -1.0;
     return ms;
+}
+
+int cmc_last_stats(cmc_ctx* ctx, uint64_t out[6]) {
+    if (!ctx || !out) return CMC_EINVAL;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    const cmc::Ctrl& s = c->last_ctrl;
+    out[0] = s.walks;
+    out[1] = s.probes;
+    out[2] = s.slot_wait_cycles;
+    out[3] = s.walker_idle_cycles;
+    out[4] = s.walker_cycles;
+    out[5] = s.error;
+    return CMC_OK;
 }
 
 uint32_t cmc_last_kernel_count(const cmc_ctx* ctx) {

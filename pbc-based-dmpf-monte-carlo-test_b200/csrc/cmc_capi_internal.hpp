@@ -40,7 +40,7 @@ struct Ctx {
     std::string err, plan_text;
     uint32_t kernels = 0;
     Plan last_plan;
-    unsigned long long last_walks = 0, last_probes = 0;
+    Ctrl last_ctrl{};
     // tuning overrides (0 = automatic)
     uint32_t force_wg = 0, force_ng = 0, force_global_slots = 0;
     int force_method = -1;  // -1 auto, 0 direct, 1 cache

@@ -110,12 +110,6 @@ __device__ __forceinline__ uint32_t claim(uint32_t* counter, bool need, uint32_t
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
-template <typename MapT, typename BinT>
-struct SlotView {
-    BinT* bins;
-    MapT* map;
-};
-
 // ---------------------------------------------------------------- producer --
 
 template <typename MapT, bool WIDE>
@@ -266,23 +260,35 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
             gh->rnd = splitmix(walk);
             gh->walk = walk;
             gh->cand_next = 0;
-            // Next slot of this group; wait until its previous walk is done.
-            const uint32_t slot = g + a.ng * (cursor % slots_per_group);
-            uint32_t spins = 0;
-            while (ld_acquire(&cs->slot_state[slot]) != kSlotFree) {
-                __nanosleep(256);
+            // Claim any free slot (FREE -> FILLING), starting from this
+            // group's share of the pool so groups rarely collide.
+            uint32_t spins = 0, slot = kMaxSlots;
+            const long long wait0 = clock64();
+            for (;;) {
+                for (uint32_t i = 0; i < a.ns; ++i) {
+                    const uint32_t sidx = (g * (a.ns / a.ng) + cursor + i) % a.ns;
+                    if (atomicCAS(&cs->slot_state[sidx], kSlotFree, kSlotFilling) == kSlotFree) {
+                        slot = sidx;
+                        break;
+                    }
+                }
+                if (slot < kMaxSlots) break;
+                __nanosleep(128);
                 if (++spins > a.spin_limit) {
                     atomicExch(&a.ctrl->error, kErrTimeout);
                     atomicExch(&a.ctrl->where, 1u);
                     gh->abort = 1;
+                    slot = 0;
                     break;
                 }
             }
             gh->slot = slot;
+            atomicAdd(&a.ctrl->slot_wait_cycles, (unsigned long long)(clock64() - wait0));
         }
         ++cursor;
         group_sync(g, gthreads);
         if (gh->abort) break;
+        __threadfence_block();  // the walker's last accesses to this slot happen-before ours
         if constexpr (!WIDE) {
             if (gt < 8) {
                 const Round1 c = round1_consts(L, gh->rk, gt, J.half_bits);
@@ -337,22 +343,61 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
 
 // ------------------------------------------------------------------ walker --
 
+// Slot storage seen by one walker lane: shared-memory offsets (loads compile
+// to shared-space instructions) or global pointers.
+template <typename MapT, typename BinT, bool SMEM>
+struct SlotMem;
+
 template <typename MapT, typename BinT>
+struct SlotMem<MapT, BinT, true> {
+    uint32_t map_off, bin_off;
+    __device__ __forceinline__ void bind(const EngineArgs& a, uint32_t slot) {
+        bin_off = a.slots_off + slot * a.slot_stride;
+        map_off = bin_off + a.bins_bytes;
+    }
+    __device__ __forceinline__ uint32_t map(uint32_t i) const {
+        return *reinterpret_cast<const MapT*>(cmc_dyn_smem + map_off + i * (uint32_t)sizeof(MapT));
+    }
+    __device__ __forceinline__ BinT bin(uint32_t i) const {
+        return *reinterpret_cast<const BinT*>(cmc_dyn_smem + bin_off + i * (uint32_t)sizeof(BinT));
+    }
+    __device__ __forceinline__ void set(uint32_t i, BinT v) const {
+        *reinterpret_cast<BinT*>(cmc_dyn_smem + bin_off + i * (uint32_t)sizeof(BinT)) = v;
+    }
+};
+
+template <typename MapT, typename BinT>
+struct SlotMem<MapT, BinT, false> {
+    const MapT* mp;
+    BinT* bp;
+    __device__ __forceinline__ void bind(const EngineArgs& a, uint32_t slot) {
+        char* base = a.gslots + ((size_t)blockIdx.x * a.ns + slot) * a.slot_stride;
+        bp = reinterpret_cast<BinT*>(base);
+        mp = reinterpret_cast<const MapT*>(base + a.bins_bytes);
+    }
+    __device__ __forceinline__ uint32_t map(uint32_t i) const { return mp[i]; }
+    __device__ __forceinline__ BinT bin(uint32_t i) const { return bp[i]; }
+    __device__ __forceinline__ void set(uint32_t i, BinT v) const { bp[i] = v; }
+};
+
+// One lane's insertion walk over a filled slot (cuckoo_core.hpp:117-161).
+// A map entry is a bucket index < B by construction (y < D = B * width);
+// any other value is recorded as an error instead of being dereferenced.
+template <typename MapT, typename BinT, bool SMEM>
 struct Walk {
     static constexpr uint32_t kShift = sizeof(BinT) == 2 ? 14 : 16;
     static constexpr uint32_t kOrdMask = (1u << kShift) - 1u;
-    static constexpr BinT kEmpty = (BinT)~(BinT)0;
+    static constexpr uint32_t kEmpty = sizeof(BinT) == 2 ? 0xffffu : 0xffffffffu;
 
-    const MapT* map;
-    BinT* bins;
+    SlotMem<MapT, BinT, SMEM> mem;
     uint64_t walk, rnd, magic;
-    uint32_t magic_shift, k, t, kick, bgh, nbins;
+    uint32_t magic_shift, k, t, kick, nbins;
     uint32_t item, cur, count, phase, choice, target;
-    bool active, failed, bad;
+    bool bgh, active, failed, bad;
 
-    __device__ __forceinline__ void begin(const Job& J, const SlotHeader& h, BinT* b, const MapT* m) {
-        map = m;
-        bins = b;
+    __device__ __forceinline__ void begin(const EngineArgs& a, uint32_t slot, const Job& J,
+                                          const SlotHeader& h) {
+        mem.bind(a, slot);
         walk = h.walk;
         rnd = h.rnd;
         k = J.k;
@@ -360,7 +405,7 @@ struct Walk {
         kick = J.kick;
         nbins = J.buckets;
         bgh = J.mode == 1;
-        // randomness / k as umulhi(rnd, magic) >> magic_shift for k in {2,3,4}
+        // rnd / k == umulhi(rnd, magic) >> magic_shift for k in {2, 3, 4}
         magic = k == 3 ? 0xAAAAAAAAAAAAAAABULL : (k == 2 ? 0x8000000000000000ULL : 0x4000000000000000ULL);
         magic_shift = k == 3 ? 1 : 0;
         item = 0; cur = 0; count = 0; phase = 0; choice = 0; target = 0;
@@ -369,119 +414,129 @@ struct Walk {
         bad = false;
     }
 
-    // A map entry is a bucket index < B by construction (y < D = B * width);
-    // anything else is recorded as an error instead of being dereferenced.
+    __device__ __forceinline__ BinT pack(uint32_t o, uint32_t j) const { return (BinT)(o | (j << kShift)); }
+
     __device__ __forceinline__ bool out_of_range(uint32_t b) {
         if (b < nbins) return false;
-        bad = true;
-        failed = true;
+        bad = failed = true;
         active = false;
         return true;
     }
 
-    __device__ __forceinline__ BinT pack(uint32_t o, uint32_t j) const { return (BinT)(o | (j << kShift)); }
-
-    // One probe of the walk.  BGH25: cuckoo_core.hpp:123-133; DRRT18: :134-158.
-    __device__ __forceinline__ void step() {
-        if (bgh) {
+    // BGH25 random walk (cuckoo_core.hpp:123-133).  The table write happens
+    // on every non-failing probe; on the failing probe the trial ends and its
+    // table is never read again, so the write is harmless and unconditional.
+    __device__ __forceinline__ void bgh_steps(int n, unsigned long long& probes) {
+#pragma unroll 1
+        for (int s = 0; s < n && active; ++s) {
             if (rnd < k) rnd = splitmix(walk);
             const uint64_t q = __umul64hi(rnd, magic) >> magic_shift;
-            const uint32_t which = (uint32_t)(rnd - q * k);
+            const uint32_t which = (uint32_t)rnd - (uint32_t)q * k;
             rnd = q;
-            const uint32_t tgt = map[cur * k + which];
-            if (out_of_range(tgt)) return;
-            const BinT old = bins[tgt];
+            const uint32_t tgt = mem.map(cur * k + which);
+            if (out_of_range(tgt)) break;
+            const uint32_t old = mem.bin(tgt);
+            mem.set(tgt, pack(cur, which));
+            ++probes;
             if (old == kEmpty) {
-                bins[tgt] = pack(cur, which);
                 cur = ++item;
                 count = 0;
-                if (item == t) active = false;
-            } else if (++count > kick) {
-                failed = true;
-                active = false;
+                active = item != t;
             } else {
-                bins[tgt] = pack(cur, which);
                 cur = old & kOrdMask;
+                if (++count > kick) {
+                    failed = true;
+                    active = false;
+                }
             }
-        } else if (phase == 0) {
-            // a new item tries its copies in order
-            const uint32_t b = map[item * k + choice];
-            if (out_of_range(b)) return;
-            if (bins[b] == kEmpty) {
-                bins[b] = pack(item, choice);
-                ++item;
-                choice = 0;
-                if (item == t) active = false;
-            } else if (++choice == k) {
-                phase = 1;
-                cur = item;
-                choice = 0;
-                target = map[item * k];
-                count = 0;
-                if (out_of_range(target)) return;
+        }
+    }
+
+    // DRRT18 cycling eviction (cuckoo_core.hpp:134-158), one probe per step.
+    __device__ __forceinline__ void drrt_steps(int n, unsigned long long& probes) {
+#pragma unroll 1
+        for (int s = 0; s < n && active; ++s) {
+            ++probes;
+            if (phase == 0) {
+                // a new item tries its copies in order
+                const uint32_t b = mem.map(item * k + choice);
+                if (out_of_range(b)) break;
+                if (mem.bin(b) == kEmpty) {
+                    mem.set(b, pack(item, choice));
+                    ++item;
+                    choice = 0;
+                    active = item != t;
+                } else if (++choice == k) {
+                    phase = 1;
+                    cur = item;
+                    choice = 0;
+                    target = mem.map(item * k);
+                    count = 0;
+                    if (out_of_range(target)) break;
+                }
+                continue;
             }
-        } else {
-            const BinT displaced = bins[target];
+            const uint32_t displaced = mem.bin(target);
             if (displaced == kEmpty) {
-                bins[target] = pack(cur, choice);
+                mem.set(target, pack(cur, choice));
                 ++item;
                 phase = 0;
                 choice = 0;
-                if (item == t) active = false;
-                return;
+                active = item != t;
+                continue;
             }
             if (count >= kick) {
                 failed = true;
                 active = false;
-                return;
+                break;
             }
-            bins[target] = pack(cur, choice);
+            mem.set(target, pack(cur, choice));
             cur = displaced & kOrdMask;
             choice = (displaced >> kShift) & 3u;
             const uint32_t previous = target;
             bool found = false;
-            for (uint32_t s = 0; s < k; ++s) {
+            for (uint32_t j = 0; j < k; ++j) {
                 choice = choice + 1 == k ? 0 : choice + 1;
-                const uint32_t next = map[cur * k + choice];
-                if (next != previous) { target = next; found = true; break; }
+                const uint32_t next = mem.map(cur * k + choice);
+                if (next != previous) {
+                    target = next;
+                    found = true;
+                    break;
+                }
             }
-            if (found && out_of_range(target)) return;
             if (!found) {
                 failed = true;
                 active = false;
-                return;
+                break;
             }
+            if (out_of_range(target)) break;
             ++count;
         }
     }
 };
 
-template <typename MapT, typename BinT>
-__device__ __forceinline__ void walker(const EngineArgs& a, char* smem, CtaShared* cs) {
+template <typename MapT, typename BinT, bool SMEM>
+__device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs) {
     const uint32_t lane = threadIdx.x & 31;
-    Walk<MapT, BinT> w;
+    Walk<MapT, BinT, SMEM> w;
     w.active = false;
+    w.bgh = true;
     bool busy = false;  // holds a slot
     unsigned long long gidx = 0;
     uint32_t job = 0;
-    unsigned long long probes = 0, walks = 0;
+    unsigned long long probes = 0, walks = 0, idle_cycles = 0;
     uint32_t idle = 0;
+    const long long born = clock64();
     for (;;) {
         if (!busy && lane < a.ns && ld_acquire(&cs->slot_state[lane]) == kSlotReady) {
             const SlotHeader h = cs->slot_hdr[lane];
-            char* sbase = a.gslots ? a.gslots + ((size_t)blockIdx.x * a.ns + lane) * a.slot_stride
-                                   : smem + a.slots_off + (size_t)lane * a.slot_stride;
             job = h.job;
             gidx = h.gidx;
-            w.begin(a.jobs[job], h, reinterpret_cast<BinT*>(sbase),
-                    reinterpret_cast<const MapT*>(sbase + a.bins_bytes));
+            w.begin(a, lane, a.jobs[job], h);
             busy = true;
         }
-#pragma unroll 1
-        for (int s = 0; s < 64 && w.active; ++s) {
-            w.step();
-            ++probes;
-        }
+        if (w.bgh) w.bgh_steps(64, probes);
+        else w.drrt_steps(64, probes);
         if (busy && !w.active) {
             if (w.bad) {
                 atomicExch(&a.ctrl->error, kErrRange);
@@ -494,6 +549,7 @@ __device__ __forceinline__ void walker(const EngineArgs& a, char* smem, CtaShare
             if (a.job_done) atomicAdd(&a.job_done[job], 1ULL);
             ++walks;
             busy = false;
+            __threadfence_block();
             st_release(&cs->slot_state[lane], kSlotFree);
         }
         if (!__any_sync(kFull, busy)) {
@@ -503,7 +559,9 @@ __device__ __forceinline__ void walker(const EngineArgs& a, char* smem, CtaShare
             const bool ready = lane < a.ns && ld_acquire(&cs->slot_state[lane]) == kSlotReady;
             if (!__any_sync(kFull, ready)) {
                 if (done) break;
+                const long long t0 = clock64();
                 __nanosleep(128);
+                idle_cycles += (unsigned long long)(clock64() - t0);
                 if (++idle > a.spin_limit) {
                     if (lane == 0) {
                         atomicExch(&a.ctrl->error, kErrTimeout);
@@ -524,6 +582,8 @@ __device__ __forceinline__ void walker(const EngineArgs& a, char* smem, CtaShare
     if (lane == 0) {
         atomicAdd(&a.ctrl->probes, probes);
         atomicAdd(&a.ctrl->walks, walks);
+        atomicAdd(&a.ctrl->walker_idle_cycles, idle_cycles);
+        atomicAdd(&a.ctrl->walker_cycles, (unsigned long long)(clock64() - born));
     }
 }
 
@@ -546,7 +606,10 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
     __syncthreads();
     const uint32_t warp = threadIdx.x >> 5;
     if (warp < a.ng * a.wg) producer<MapT, BinT, WIDE>(a, smem, cs, warp / a.wg);
-    else if (warp == a.ng * a.wg) walker<MapT, BinT>(a, smem, cs);
+    else if (warp == a.ng * a.wg) {
+        if (a.gslots) walker<MapT, BinT, false>(a, cs);
+        else walker<MapT, BinT, true>(a, cs);
+    }
 }
 
 // Ordered failure list from the bitmap: one CTA, block-wide exclusive scan.

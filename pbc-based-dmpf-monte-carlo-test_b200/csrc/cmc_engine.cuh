@@ -10,6 +10,7 @@ constexpr uint32_t kMethodCache = 1;   // 8*2^h round cache in shared memory, th
 
 constexpr uint32_t kSlotFree = 0;
 constexpr uint32_t kSlotReady = 1;
+constexpr uint32_t kSlotFilling = 2;
 
 constexpr uint32_t kMaxSlots = 32;  // one walker lane per slot
 constexpr uint32_t kEngineTableBytes = 65536;  // replicated T-table at shared offset 0
@@ -36,6 +37,9 @@ struct Ctrl {
     unsigned int where;        // which wait gave up (diagnostics)
     unsigned long long walks;  // walks completed (all jobs)
     unsigned long long probes; // probes spent (all jobs)
+    unsigned long long slot_wait_cycles;   // producer leaders waiting for a free slot
+    unsigned long long walker_idle_cycles; // walker warps with no slot to walk
+    unsigned long long walker_cycles;      // walker warps' lifetime
 };
 
 struct EngineArgs {
