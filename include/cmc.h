@@ -94,8 +94,9 @@ int cmc_check(cmc_ctx* ctx);
 /* Tuning knobs of the launch planner; value 0 (or -1 for "method") restores
  * the automatic choice.  Names: "warps_per_group" (1..15), "groups" (1..14),
  * "global_slots" (0/1: keep walk slots in global memory), "method"
- * (-1 auto, 0 direct AES passes, 1 shared-memory round cache), "spin_limit"
- * (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown
+ * (-1 auto, 0 direct AES passes, 1 shared-memory round cache), "walkers"
+ * (1..2 walker warps), "slots_per_group" (cap on shared-memory slots per
+ * group, default 8), "spin_limit" (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown
  * name or a value out of range. */
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
 

@@ -133,7 +133,8 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     const double avg_cand = work > 0 ? cand_work / work : 0;
     pl.wg = (any_cache || avg_cand >= 768.0) ? 4 : 1;
     if (force_wg) pl.wg = force_wg;
-    const uint32_t max_producer_warps = 15;
+    pl.nw = force_walkers ? force_walkers : 1;
+    const uint32_t max_producer_warps = 16 - pl.nw;
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
     uint32_t ng = std::min<uint32_t>(kMaxGroups, max_producer_warps / pl.wg);
     if (force_ng) ng = std::min(ng, force_ng);
@@ -145,7 +146,8 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.slots_smem = false;
     for (uint32_t g = ng; !force_global_slots && g >= std::max<uint32_t>(1, (ng + 1) / 2); --g) {
         const uint32_t left = budget - g * pl.group_bytes;
-        const uint32_t s = std::min<uint32_t>({left / pl.slot_stride / g, kMaxSlots / g, 4u});
+        const uint32_t s = std::min<uint32_t>({left / pl.slot_stride / g, kMaxSlots / g,
+                                               max_slots_per_group});
         if (s >= 2) {
             pl.ng = g;
             pl.ns = g * s;
@@ -160,14 +162,14 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.group_off = kEngineTableBytes + kCtaSharedBytes;
     pl.slots_off = pl.group_off + pl.ng * pl.group_bytes;
     pl.smem_bytes = pl.slots_off + (pl.slots_smem ? pl.ns * pl.slot_stride : 0);
-    pl.threads = (pl.ng * pl.wg + 1) * 32;
+    pl.threads = (pl.ng * pl.wg + pl.nw) * 32;
     pl.ctas = sms;
     char buf[256];
     snprintf(buf, sizeof buf,
-             "engine=group variant=%s groups=%u warps_per_group=%u slots=%u slots_in=%s "
+             "engine=group variant=%s groups=%u warps_per_group=%u walkers=%u slots=%u slots_in=%s "
              "smem=%u threads=%u ctas=%u cache=%s",
              pl.variant == 0 ? "narrow" : pl.variant == 1 ? "wide" : "wide-domain", pl.ng, pl.wg,
-             pl.ns, pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
+             pl.nw, pl.ns, pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
              any_cache ? "on" : "off");
     plan_text = buf;
     return CMC_OK;
@@ -204,6 +206,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     a.ng = pl.ng;
     a.wg = pl.wg;
     a.ns = pl.ns;
+    a.nw = pl.nw;
     a.group_bytes = pl.group_bytes;
     a.group_off = pl.group_off;
     a.slots_off = pl.slots_off;
@@ -415,6 +418,9 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "groups" && value >= 0 && value <= cmc::kMaxGroups) c->force_ng = uint32_t(value);
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
     else if (n == "method" && value >= -1 && value <= 1) c->force_method = int(value);
+    else if (n == "walkers" && value >= 0 && value <= 2) c->force_walkers = uint32_t(value);
+    else if (n == "slots_per_group" && value >= 0 && value <= 32)
+        c->max_slots_per_group = value ? uint32_t(value) : 8u;
     else if (n == "spin_limit" && value >= 0 && value <= 0xffffffffLL)
         c->spin_limit = value ? uint32_t(value) : (1u << 26);
     else return c->fail(CMC_EINVAL, "unknown option or value out of range: %s=%lld", name, (long long)value);

@@ -390,8 +390,8 @@ struct Walk {
     static constexpr uint32_t kEmpty = sizeof(BinT) == 2 ? 0xffffu : 0xffffffffu;
 
     SlotMem<MapT, BinT, SMEM> mem;
-    uint64_t walk, rnd, magic;
-    uint32_t magic_shift, k, t, kick, nbins;
+    uint64_t walk, rnd, magic, digits;
+    uint32_t magic_shift, k, t, kick, nbins, ndigits;
     uint32_t item, cur, count, phase, choice, target;
     bool bgh, active, failed, bad;
 
@@ -409,6 +409,8 @@ struct Walk {
         magic = k == 3 ? 0xAAAAAAAAAAAAAAABULL : (k == 2 ? 0x8000000000000000ULL : 0x4000000000000000ULL);
         magic_shift = k == 3 ? 1 : 0;
         item = 0; cur = 0; count = 0; phase = 0; choice = 0; target = 0;
+        digits = 0;
+        ndigits = 0;
         active = true;
         failed = false;
         bad = false;
@@ -423,32 +425,49 @@ struct Walk {
         return true;
     }
 
+    // The next 32 base-k digits of the walk's randomness, exactly as the
+    // reference consumes them one per probe ("if (r < k) r = splitmix(walk);
+    // which = r % k; r /= k", cuckoo_core.hpp:126-127), packed 2 bits each.
+    // The stream does not depend on the table, so it is decoded ahead of the
+    // probes and stays off their load-to-load dependency chain.
+    __device__ __forceinline__ void refill_digits() {
+        uint64_t d = 0;
+#pragma unroll 4
+        for (uint32_t i = 0; i < 32; ++i) {
+            if (rnd < k) rnd = splitmix(walk);
+            const uint64_t q = __umul64hi(rnd, magic) >> magic_shift;
+            d |= (uint64_t)((uint32_t)rnd - (uint32_t)q * k) << (2 * i);
+            rnd = q;
+        }
+        digits = d;
+        ndigits = 32;
+    }
+
     // BGH25 random walk (cuckoo_core.hpp:123-133).  The table write happens
     // on every non-failing probe; on the failing probe the trial ends and its
     // table is never read again, so the write is harmless and unconditional.
     __device__ __forceinline__ void bgh_steps(int n, unsigned long long& probes) {
 #pragma unroll 1
         for (int s = 0; s < n && active; ++s) {
-            if (rnd < k) rnd = splitmix(walk);
-            const uint64_t q = __umul64hi(rnd, magic) >> magic_shift;
-            const uint32_t which = (uint32_t)rnd - (uint32_t)q * k;
-            rnd = q;
-            const uint32_t tgt = mem.map(cur * k + which);
-            if (out_of_range(tgt)) break;
+            if (ndigits == 0) refill_digits();
+            const uint32_t which = (uint32_t)digits & 3u;
+            digits >>= 2;
+            --ndigits;
+            uint32_t tgt = mem.map(cur * k + which);
+            if (tgt >= nbins) {
+                bad = true;
+                tgt = 0;
+            }
             const uint32_t old = mem.bin(tgt);
             mem.set(tgt, pack(cur, which));
             ++probes;
-            if (old == kEmpty) {
-                cur = ++item;
-                count = 0;
-                active = item != t;
-            } else {
-                cur = old & kOrdMask;
-                if (++count > kick) {
-                    failed = true;
-                    active = false;
-                }
-            }
+            const bool empty = old == kEmpty;
+            item += empty;
+            count = empty ? 0 : count + 1;
+            cur = empty ? item : (old & kOrdMask);
+            const bool fail = count > kick || bad;
+            failed = fail;
+            active = !fail && item != t;
         }
     }
 
@@ -516,8 +535,10 @@ struct Walk {
 };
 
 template <typename MapT, typename BinT, bool SMEM>
-__device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs) {
+__device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint32_t wi) {
     const uint32_t lane = threadIdx.x & 31;
+    const uint32_t my = lane * a.nw + wi;  // this lane's slot
+    const bool owner = my < a.ns;
     Walk<MapT, BinT, SMEM> w;
     w.active = false;
     w.bgh = true;
@@ -528,11 +549,11 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs) {
     uint32_t idle = 0;
     const long long born = clock64();
     for (;;) {
-        if (!busy && lane < a.ns && ld_acquire(&cs->slot_state[lane]) == kSlotReady) {
-            const SlotHeader h = cs->slot_hdr[lane];
+        if (!busy && owner && ld_acquire(&cs->slot_state[my]) == kSlotReady) {
+            const SlotHeader h = cs->slot_hdr[my];
             job = h.job;
             gidx = h.gidx;
-            w.begin(a, lane, a.jobs[job], h);
+            w.begin(a, my, a.jobs[job], h);
             busy = true;
         }
         if (w.bgh) w.bgh_steps(64, probes);
@@ -550,13 +571,13 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs) {
             ++walks;
             busy = false;
             __threadfence_block();
-            st_release(&cs->slot_state[lane], kSlotFree);
+            st_release(&cs->slot_state[my], kSlotFree);
         }
         if (!__any_sync(kFull, busy)) {
             // Every lane acquires groups_done itself; the warp leaves only when
             // all lanes saw every group finished and no slot is still READY.
             const bool done = __all_sync(kFull, ld_acquire(&cs->groups_done) == a.ng);
-            const bool ready = lane < a.ns && ld_acquire(&cs->slot_state[lane]) == kSlotReady;
+            const bool ready = owner && ld_acquire(&cs->slot_state[my]) == kSlotReady;
             if (!__any_sync(kFull, ready)) {
                 if (done) break;
                 const long long t0 = clock64();
@@ -606,9 +627,10 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
     __syncthreads();
     const uint32_t warp = threadIdx.x >> 5;
     if (warp < a.ng * a.wg) producer<MapT, BinT, WIDE>(a, smem, cs, warp / a.wg);
-    else if (warp == a.ng * a.wg) {
-        if (a.gslots) walker<MapT, BinT, false>(a, cs);
-        else walker<MapT, BinT, true>(a, cs);
+    else if (warp < a.ng * a.wg + a.nw) {
+        const uint32_t wi = warp - a.ng * a.wg;
+        if (a.gslots) walker<MapT, BinT, false>(a, cs, wi);
+        else walker<MapT, BinT, true>(a, cs, wi);
     }
 }
 

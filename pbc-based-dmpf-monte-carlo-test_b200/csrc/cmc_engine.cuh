@@ -55,6 +55,7 @@ struct EngineArgs {
     uint32_t slot_stride;               // bytes per slot
     uint32_t bins_bytes;                // map starts this far into a slot
     uint32_t ng, wg, ns;                // groups, warps per group, slots
+    uint32_t nw;                        // walker warps (slot s -> walker s % nw)
     uint32_t group_bytes;               // per-group smem (header + cache)
     uint32_t group_off;                 // smem offset of group 0
     uint32_t slots_off;                 // smem offset of slot 0 (smem slots)
