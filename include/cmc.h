@@ -96,7 +96,9 @@ int cmc_check(cmc_ctx* ctx);
  * "global_slots" (0/1: keep walk slots in global memory), "method"
  * (-1 auto, 0 direct AES passes, 1 shared-memory round cache), "walkers"
  * (1..2 walker warps), "slots_per_group" (cap on shared-memory slots per
- * group, default 8), "spin_limit" (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown
+ * group, default 8), "walker_ctas" (-1 auto, 0 walks inside each CTA, N > 0
+ * dedicates N CTAs -- one per SM -- to walks over global slots while the
+ * others only build maps), "spin_limit" (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown
  * name or a value out of range. */
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
 

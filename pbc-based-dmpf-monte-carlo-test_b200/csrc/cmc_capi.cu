@@ -19,6 +19,8 @@ namespace cmc {
 
 template <typename MapT, typename BinT, bool WIDE>
 __global__ void cmc_engine(const EngineArgs a);
+template <typename MapT, typename BinT, bool WIDE>
+__global__ void cmc_engine_split(const EngineArgs a);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
                                      uint32_t* out, uint32_t* count);
 __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out);
@@ -133,7 +135,9 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     const double avg_cand = work > 0 ? cand_work / work : 0;
     pl.wg = (any_cache || avg_cand >= 768.0) ? 4 : 1;
     if (force_wg) pl.wg = force_wg;
-    pl.nw = force_walkers ? force_walkers : 1;
+    pl.walker_ctas = force_walker_ctas > 0 ? uint32_t(force_walker_ctas) : 0;
+    if (pl.walker_ctas >= uint32_t(sms)) return fail(CMC_EINVAL, "walker_ctas must be below the SM count");
+    pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : 1);
     const uint32_t max_producer_warps = 16 - pl.nw;
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
     uint32_t ng = std::min<uint32_t>(kMaxGroups, max_producer_warps / pl.wg);
@@ -141,10 +145,12 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     while (ng > 1 && ng * pl.group_bytes > budget) --ng;
     if (ng * pl.group_bytes > budget)
         return fail(CMC_EINVAL, "round cache of %u bytes does not fit shared memory", cache_bytes);
-    // Slots: 2..4 per group in shared memory when that fits without giving up
+    // Slots: 2..8 per group in shared memory when that fits without giving up
     // more than half of the groups; otherwise up to 32 in global memory.
+    // The split engine keeps one global slot per walker-CTA thread.
     pl.slots_smem = false;
-    for (uint32_t g = ng; !force_global_slots && g >= std::max<uint32_t>(1, (ng + 1) / 2); --g) {
+    for (uint32_t g = ng; !pl.walker_ctas && !force_global_slots &&
+                          g >= std::max<uint32_t>(1, (ng + 1) / 2); --g) {
         const uint32_t left = budget - g * pl.group_bytes;
         const uint32_t s = std::min<uint32_t>({left / pl.slot_stride / g, kMaxSlots / g,
                                                max_slots_per_group});
@@ -155,7 +161,10 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
             break;
         }
     }
-    if (!pl.slots_smem) {
+    if (pl.walker_ctas) {
+        pl.ng = ng;
+        pl.ns = pl.walker_ctas * pl.ng * pl.wg * 32;
+    } else if (!pl.slots_smem) {
         pl.ng = ng;
         pl.ns = std::max<uint32_t>(1, kMaxSlots / ng) * ng;
     }
@@ -166,10 +175,10 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.ctas = sms;
     char buf[256];
     snprintf(buf, sizeof buf,
-             "engine=group variant=%s groups=%u warps_per_group=%u walkers=%u slots=%u slots_in=%s "
+             "engine=%s variant=%s groups=%u warps_per_group=%u walkers=%u slots=%u slots_in=%s "
              "smem=%u threads=%u ctas=%u cache=%s",
-             pl.variant == 0 ? "narrow" : pl.variant == 1 ? "wide" : "wide-domain", pl.ng, pl.wg,
-             pl.nw, pl.ns, pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
+             pl.walker_ctas ? "split" : "group", pl.variant == 0 ? "narrow" : pl.variant == 1 ? "wide" : "wide-domain", pl.ng, pl.wg,
+             pl.walker_ctas ? pl.walker_ctas : pl.nw, pl.ns, pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
              any_cache ? "on" : "off");
     plan_text = buf;
     return CMC_OK;
@@ -185,7 +194,12 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     if (rc) return rc;
     const size_t words = (total + 31) / 32;
     if ((rc = grow(d_bits, bits_cap, words, "failure bitmap"))) return rc;
-    if (!pl.slots_smem) {
+    if (pl.walker_ctas) {
+        if ((rc = grow(d_slots, slots_cap, size_t(pl.ns) * pl.slot_stride, "slot pool"))) return rc;
+        if ((rc = grow(d_ghdr, ghdr_cap, pl.ns, "slot headers"))) return rc;
+        if ((rc = cuda(cudaMemsetAsync(d_ghdr, 0, size_t(pl.ns) * sizeof(GSlotHeader), st), "memset slots")))
+            return rc;
+    } else if (!pl.slots_smem) {
         const size_t need = size_t(pl.ctas) * pl.ns * pl.slot_stride;
         if ((rc = grow(d_slots, slots_cap, need, "slot pool"))) return rc;
     }
@@ -200,6 +214,10 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     a.job_failed = job_failed;
     a.job_done = job_done;
     a.gslots = pl.slots_smem ? nullptr : d_slots;
+    a.ghdr = pl.walker_ctas ? d_ghdr : nullptr;
+    a.split = pl.walker_ctas ? 1 : 0;
+    a.producer_ctas = pl.ctas - pl.walker_ctas;
+    a.total_groups = a.producer_ctas * pl.ng;
     a.t0 = d_t0;
     a.slot_stride = pl.slot_stride;
     a.bins_bytes = pl.bins_bytes;
@@ -211,16 +229,26 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     a.group_off = pl.group_off;
     a.slots_off = pl.slots_off;
     a.spin_limit = spin_limit;
-    const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
-                   : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
-                                     : (const void*)cmc_engine<uint32_t, uint32_t, true>;
+    const void* fn =
+        pl.walker_ctas
+            ? (pl.variant == 0   ? (const void*)cmc_engine_split<uint16_t, uint16_t, false>
+               : pl.variant == 1 ? (const void*)cmc_engine_split<uint32_t, uint32_t, false>
+                                 : (const void*)cmc_engine_split<uint32_t, uint32_t, true>)
+            : (pl.variant == 0   ? (const void*)cmc_engine<uint16_t, uint16_t, false>
+               : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
+                                 : (const void*)cmc_engine<uint32_t, uint32_t, true>);
     if ((rc = cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         int(pl.smem_bytes)),
                    "cudaFuncSetAttribute")))
         return rc;
     void* args[] = {&a};
     if ((rc = cuda(cudaEventRecord(ev_start, st), "event"))) return rc;
-    if ((rc = cuda(cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, st),
+    // The split engine's producer and walker CTAs hand trials to each other, so
+    // they must all be resident at once: a cooperative launch guarantees it.
+    if ((rc = cuda(pl.walker_ctas ? cudaLaunchCooperativeKernel(fn, dim3(pl.ctas), dim3(pl.threads),
+                                                                 args, pl.smem_bytes, st)
+                                  : cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args,
+                                                     pl.smem_bytes, st),
                    "engine launch")))
         return rc;
     if ((rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
@@ -294,6 +322,7 @@ Ctx::~Ctx() {
     cudaFree(d_bits);
     cudaFree(d_out);
     cudaFree(d_slots);
+    cudaFree(d_ghdr);
     cudaFree(d_key);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
@@ -419,6 +448,7 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
     else if (n == "method" && value >= -1 && value <= 1) c->force_method = int(value);
     else if (n == "walkers" && value >= 0 && value <= 2) c->force_walkers = uint32_t(value);
+    else if (n == "walker_ctas" && value >= -1 && value < c->sms) c->force_walker_ctas = int(value);
     else if (n == "slots_per_group" && value >= 0 && value <= 32)
         c->max_slots_per_group = value ? uint32_t(value) : 8u;
     else if (n == "spin_limit" && value >= 0 && value <= 0xffffffffLL)

@@ -69,6 +69,16 @@ __device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
                  : "memory");
 }
 
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ void group_sync(uint32_t g, uint32_t nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(nthreads) : "memory");
 }
@@ -218,7 +228,7 @@ __device__ __forceinline__ void build_map_cache(const Job& J, GroupHeader* gh,
     }
 }
 
-template <typename MapT, typename BinT, bool WIDE>
+template <typename MapT, typename BinT, bool WIDE, bool SPLIT>
 __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaShared* cs, uint32_t g) {
     const uint32_t gthreads = a.wg * 32;
     const uint32_t gt = threadIdx.x - g * gthreads;
@@ -260,19 +270,26 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
             gh->rnd = splitmix(walk);
             gh->walk = walk;
             gh->cand_next = 0;
-            // Claim any free slot (FREE -> FILLING), starting from this
-            // group's share of the pool so groups rarely collide.
-            uint32_t spins = 0, slot = kMaxSlots;
+            // Claim a free slot (FREE -> FILLING).  In-CTA slots: any free
+            // one, starting from this group's share of the pool.  Split
+            // engine: the next slot of a global ring, waiting for its walk.
+            uint32_t spins = 0, slot = 0xffffffffu;
             const long long wait0 = clock64();
+            uint32_t ring = 0;
+            if constexpr (SPLIT) ring = atomicAdd(&a.ctrl->slot_cursor, 1u) % a.ns;
             for (;;) {
-                for (uint32_t i = 0; i < a.ns; ++i) {
-                    const uint32_t sidx = (g * (a.ns / a.ng) + cursor + i) % a.ns;
-                    if (atomicCAS(&cs->slot_state[sidx], kSlotFree, kSlotFilling) == kSlotFree) {
-                        slot = sidx;
-                        break;
+                if constexpr (SPLIT) {
+                    if (atomicCAS(&a.ghdr[ring].state, kSlotFree, kSlotFilling) == kSlotFree) slot = ring;
+                } else {
+                    for (uint32_t i = 0; i < a.ns; ++i) {
+                        const uint32_t sidx = (g * (a.ns / a.ng) + cursor + i) % a.ns;
+                        if (atomicCAS(&cs->slot_state[sidx], kSlotFree, kSlotFilling) == kSlotFree) {
+                            slot = sidx;
+                            break;
+                        }
                     }
                 }
-                if (slot < kMaxSlots) break;
+                if (slot != 0xffffffffu) break;
                 __nanosleep(128);
                 if (++spins > a.spin_limit) {
                     atomicExch(&a.ctrl->error, kErrTimeout);
@@ -288,7 +305,9 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         ++cursor;
         group_sync(g, gthreads);
         if (gh->abort) break;
-        __threadfence_block();  // the walker's last accesses to this slot happen-before ours
+        // the walker's last accesses to this slot happen-before ours
+        if constexpr (SPLIT) __threadfence();
+        else __threadfence_block();
         if constexpr (!WIDE) {
             if (gt < 8) {
                 const Round1 c = round1_consts(L, gh->rk, gt, J.half_bits);
@@ -299,8 +318,9 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         group_sync(g, gthreads);
 
         const uint32_t slot = gh->slot;
-        char* sbase = a.gslots ? a.gslots + ((size_t)blockIdx.x * a.ns + slot) * a.slot_stride
-                               : smem + a.slots_off + (size_t)slot * a.slot_stride;
+        char* sbase = SPLIT    ? a.gslots + (size_t)slot * a.slot_stride
+                      : a.gslots ? a.gslots + ((size_t)blockIdx.x * a.ns + slot) * a.slot_stride
+                                 : smem + a.slots_off + (size_t)slot * a.slot_stride;
         BinT* bins = reinterpret_cast<BinT*>(sbase);
         MapT* map = reinterpret_cast<MapT*>(sbase + a.bins_bytes);
         {
@@ -323,21 +343,38 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         } else {
             build_map_direct<MapT, WIDE>(L, J, gh, key, map, lane);
         }
-        __threadfence_block();
+        if constexpr (SPLIT) __threadfence();
+        else __threadfence_block();
         group_sync(g, gthreads);
         if (gt == 0) {
-            SlotHeader& sh = cs->slot_hdr[slot];
-            sh.gidx = gi;
-            sh.walk = gh->walk;
-            sh.rnd = gh->rnd;
-            sh.job = gh->job;
-            sh.offset = gh->offset;
-            st_release(&cs->slot_state[slot], kSlotReady);
+            if constexpr (SPLIT) {
+                GSlotHeader& sh = a.ghdr[slot];
+                sh.gidx = gi;
+                sh.walk = gh->walk;
+                sh.rnd = gh->rnd;
+                sh.job = gh->job;
+                sh.offset = gh->offset;
+                __threadfence();
+                st_release_gpu(&sh.state, kSlotReady);
+            } else {
+                SlotHeader& sh = cs->slot_hdr[slot];
+                sh.gidx = gi;
+                sh.walk = gh->walk;
+                sh.rnd = gh->rnd;
+                sh.job = gh->job;
+                sh.offset = gh->offset;
+                st_release(&cs->slot_state[slot], kSlotReady);
+            }
         }
     }
     if (gt == 0) {
-        __threadfence_block();
-        atomicAdd(&cs->groups_done, 1u);
+        if constexpr (SPLIT) {
+            __threadfence();
+            atomicAdd(&a.ctrl->groups_done, 1u);
+        } else {
+            __threadfence_block();
+            atomicAdd(&cs->groups_done, 1u);
+        }
     }
 }
 
@@ -366,18 +403,20 @@ struct SlotMem<MapT, BinT, true> {
     }
 };
 
+// Global slots are read and written at L2 (ld/st .cg): a slot is refilled by
+// another thread, possibly on another SM, so no stale L1 line may serve it.
 template <typename MapT, typename BinT>
 struct SlotMem<MapT, BinT, false> {
     const MapT* mp;
     BinT* bp;
     __device__ __forceinline__ void bind(const EngineArgs& a, uint32_t slot) {
-        char* base = a.gslots + ((size_t)blockIdx.x * a.ns + slot) * a.slot_stride;
+        char* base = a.gslots + (a.split ? (size_t)slot : ((size_t)blockIdx.x * a.ns + slot)) * a.slot_stride;
         bp = reinterpret_cast<BinT*>(base);
         mp = reinterpret_cast<const MapT*>(base + a.bins_bytes);
     }
-    __device__ __forceinline__ uint32_t map(uint32_t i) const { return mp[i]; }
-    __device__ __forceinline__ BinT bin(uint32_t i) const { return bp[i]; }
-    __device__ __forceinline__ void set(uint32_t i, BinT v) const { bp[i] = v; }
+    __device__ __forceinline__ uint32_t map(uint32_t i) const { return __ldcg(mp + i); }
+    __device__ __forceinline__ BinT bin(uint32_t i) const { return __ldcg(bp + i); }
+    __device__ __forceinline__ void set(uint32_t i, BinT v) const { __stcg(bp + i, v); }
 };
 
 // One lane's insertion walk over a filled slot (cuckoo_core.hpp:117-161).
@@ -608,7 +647,105 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
     }
 }
 
+// Split engine walker: every thread of a walker CTA owns one global slot.
+template <typename MapT, typename BinT>
+__device__ __forceinline__ void walker_split(const EngineArgs& a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t my = (blockIdx.x - a.producer_ctas) * blockDim.x + threadIdx.x;
+    const bool owner = my < a.ns;
+    GSlotHeader* hdr = owner ? &a.ghdr[my] : a.ghdr;
+    Walk<MapT, BinT, false> w;
+    w.active = false;
+    w.bgh = true;
+    bool busy = false;
+    unsigned long long gidx = 0;
+    uint32_t job = 0;
+    unsigned long long probes = 0, walks = 0, idle_cycles = 0;
+    uint32_t idle = 0;
+    const long long born = clock64();
+    for (;;) {
+        if (!busy && owner && ld_acquire_gpu(&hdr->state) == kSlotReady) {
+            SlotHeader h;
+            h.gidx = __ldcg(&hdr->gidx);
+            h.walk = __ldcg(&hdr->walk);
+            h.rnd = __ldcg(&hdr->rnd);
+            h.job = __ldcg(&hdr->job);
+            h.offset = __ldcg(&hdr->offset);
+            job = h.job;
+            gidx = h.gidx;
+            w.begin(a, my, a.jobs[job], h);
+            busy = true;
+        }
+        if (w.bgh) w.bgh_steps(64, probes);
+        else w.drrt_steps(64, probes);
+        if (busy && !w.active) {
+            if (w.bad) {
+                atomicExch(&a.ctrl->error, kErrRange);
+                atomicExch(&a.ctrl->where, 3u);
+            }
+            if (w.failed) {
+                atomicOr(&a.fail_bits[gidx >> 5], 1u << (gidx & 31));
+                if (a.job_failed) atomicAdd(&a.job_failed[job], 1ULL);
+            }
+            if (a.job_done) atomicAdd(&a.job_done[job], 1ULL);
+            ++walks;
+            busy = false;
+            __threadfence();
+            st_release_gpu(&hdr->state, kSlotFree);
+        }
+        if (!__any_sync(kFull, busy)) {
+            const bool done = __all_sync(kFull, ld_acquire_gpu(&a.ctrl->groups_done) == a.total_groups);
+            const bool ready = owner && ld_acquire_gpu(&hdr->state) == kSlotReady;
+            if (!__any_sync(kFull, ready)) {
+                if (done) break;
+                const long long t0 = clock64();
+                __nanosleep(256);
+                idle_cycles += (unsigned long long)(clock64() - t0);
+                if (++idle > a.spin_limit) {
+                    if (lane == 0) {
+                        atomicExch(&a.ctrl->error, kErrTimeout);
+                        atomicExch(&a.ctrl->where, 4u);
+                    }
+                    break;
+                }
+            }
+        } else {
+            idle = 0;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        probes += __shfl_xor_sync(kFull, probes, o);
+        walks += __shfl_xor_sync(kFull, walks, o);
+        idle_cycles += __shfl_xor_sync(kFull, idle_cycles, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&a.ctrl->probes, probes);
+        atomicAdd(&a.ctrl->walks, walks);
+        atomicAdd(&a.ctrl->walker_idle_cycles, idle_cycles / 32);
+        atomicAdd(&a.ctrl->walker_cycles, (unsigned long long)(clock64() - born));
+    }
+}
+
 }  // namespace
+
+template <typename MapT, typename BinT, bool WIDE>
+__global__ void __launch_bounds__(512, 1) cmc_engine_split(const EngineArgs a) {
+    if (blockIdx.x >= a.producer_ctas) {
+        walker_split<MapT, BinT>(a);
+        return;
+    }
+    char* smem = cmc_dyn_smem;
+    {
+        uint32_t* tw = reinterpret_cast<uint32_t*>(smem);
+        for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) {
+            const uint32_t v = __ldg(&a.t0[i >> 6]);
+            tw[i] = (i & 32) ? __funnelshift_r(v, v, 16) : v;
+        }
+    }
+    __syncthreads();
+    const uint32_t warp = threadIdx.x >> 5;
+    if (warp < a.ng * a.wg) producer<MapT, BinT, WIDE, true>(a, smem, nullptr, warp / a.wg);
+}
 
 template <typename MapT, typename BinT, bool WIDE>
 __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
@@ -626,7 +763,7 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
     if (threadIdx.x == 0) cs->groups_done = 0;
     __syncthreads();
     const uint32_t warp = threadIdx.x >> 5;
-    if (warp < a.ng * a.wg) producer<MapT, BinT, WIDE>(a, smem, cs, warp / a.wg);
+    if (warp < a.ng * a.wg) producer<MapT, BinT, WIDE, false>(a, smem, cs, warp / a.wg);
     else if (warp < a.ng * a.wg + a.nw) {
         const uint32_t wi = warp - a.ng * a.wg;
         if (a.gslots) walker<MapT, BinT, false>(a, cs, wi);
@@ -721,5 +858,8 @@ __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32
 template __global__ void cmc_engine<uint16_t, uint16_t, false>(const EngineArgs);
 template __global__ void cmc_engine<uint32_t, uint32_t, false>(const EngineArgs);
 template __global__ void cmc_engine<uint32_t, uint32_t, true>(const EngineArgs);
+template __global__ void cmc_engine_split<uint16_t, uint16_t, false>(const EngineArgs);
+template __global__ void cmc_engine_split<uint32_t, uint32_t, false>(const EngineArgs);
+template __global__ void cmc_engine_split<uint32_t, uint32_t, true>(const EngineArgs);
 
 }  // namespace cmc

@@ -40,6 +40,15 @@ struct Ctrl {
     unsigned long long slot_wait_cycles;   // producer leaders waiting for a free slot
     unsigned long long walker_idle_cycles; // walker warps with no slot to walk
     unsigned long long walker_cycles;      // walker warps' lifetime
+    unsigned int slot_cursor;              // split engine: next slot to try
+    unsigned int groups_done;              // split engine: producer groups finished
+};
+
+// Split engine: header of one global slot (one walker thread per slot).
+struct __align__(64) GSlotHeader {
+    unsigned long long gidx, walk, rnd;
+    uint32_t job, offset;
+    uint32_t state;  // kSlotFree / kSlotFilling / kSlotReady
 };
 
 struct EngineArgs {
@@ -56,6 +65,10 @@ struct EngineArgs {
     uint32_t bins_bytes;                // map starts this far into a slot
     uint32_t ng, wg, ns;                // groups, warps per group, slots
     uint32_t nw;                        // walker warps (slot s -> walker s % nw)
+    // split engine: CTAs [0, producer_ctas) produce maps, the rest walk; slot s
+    // is walked by thread s of the walker CTAs; headers in global memory
+    GSlotHeader* ghdr;
+    uint32_t split, producer_ctas, total_groups;
     uint32_t group_bytes;               // per-group smem (header + cache)
     uint32_t group_off;                 // smem offset of group 0
     uint32_t slots_off;                 // smem offset of slot 0 (smem slots)
