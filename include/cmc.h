@@ -95,7 +95,8 @@ int cmc_check(cmc_ctx* ctx);
  * the automatic choice.  Names: "warps_per_group" (1..15), "groups" (1..14),
  * "global_slots" (0/1: keep walk slots in global memory), "method"
  * (-1 auto, 0 direct AES passes, 1 shared-memory round cache), "walkers"
- * (1..2 walker warps), "slots_per_group" (cap on shared-memory slots per
+ * (1..4 walker warps), "isolate_walkers" (-1 auto, 0/1: walker warps alone
+ * on SM sub-partition 3, producers on 0..2), "slots_per_group" (cap on shared-memory slots per
  * group, default 8), "walker_ctas" (-1 auto, 0 walks inside each CTA, N > 0
  * dedicates N CTAs -- one per SM -- to walks over global slots while the
  * others only build maps), "spin_limit" (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown

@@ -137,8 +137,16 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     if (force_wg) pl.wg = force_wg;
     pl.walker_ctas = force_walker_ctas > 0 ? uint32_t(force_walker_ctas) : 0;
     if (pl.walker_ctas >= uint32_t(sms)) return fail(CMC_EINVAL, "walker_ctas must be below the SM count");
-    pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : 1);
-    const uint32_t max_producer_warps = 16 - pl.nw;
+    // Isolated walkers (sub-partition 3 only) pay off when walks are long
+    // enough to hold producers back; short walks keep all 16 warps busy.
+    double avg_probe_work = 0;
+    for (const Job& j : jobs) avg_probe_work += double(j.count) * j.pnum;
+    avg_probe_work = work > 0 ? avg_probe_work / work : 0;
+    pl.isolate = pl.walker_ctas ? 0 : (force_isolate >= 0 ? uint32_t(force_isolate)
+                                                          : (avg_probe_work >= 512 ? 1u : 0u));
+    pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : (pl.isolate ? 2 : 1));
+    if (pl.isolate && pl.nw > 4) pl.nw = 4;
+    const uint32_t max_producer_warps = pl.isolate ? 12 : 16 - pl.nw;
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
     uint32_t ng = std::min<uint32_t>(kMaxGroups, max_producer_warps / pl.wg);
     if (force_ng) ng = std::min(ng, force_ng);
@@ -171,14 +179,22 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.group_off = kEngineTableBytes + kCtaSharedBytes;
     pl.slots_off = pl.group_off + pl.ng * pl.group_bytes;
     pl.smem_bytes = pl.slots_off + (pl.slots_smem ? pl.ns * pl.slot_stride : 0);
-    pl.threads = (pl.ng * pl.wg + pl.nw) * 32;
+    if (pl.isolate) {
+        const uint32_t P = pl.ng * pl.wg;
+        const uint32_t last_producer_warp = P ? (P - 1) + (P - 1) / 3 : 0;
+        const uint32_t last_walker_warp = pl.nw ? 4 * (pl.nw - 1) + 3 : 0;
+        pl.threads = (std::max(last_producer_warp, last_walker_warp) + 1) * 32;
+    } else {
+        pl.threads = (pl.ng * pl.wg + pl.nw) * 32;
+    }
     pl.ctas = sms;
     char buf[256];
     snprintf(buf, sizeof buf,
-             "engine=%s variant=%s groups=%u warps_per_group=%u walkers=%u slots=%u slots_in=%s "
+             "engine=%s variant=%s groups=%u warps_per_group=%u walkers=%u%s slots=%u slots_in=%s "
              "smem=%u threads=%u ctas=%u cache=%s",
              pl.walker_ctas ? "split" : "group", pl.variant == 0 ? "narrow" : pl.variant == 1 ? "wide" : "wide-domain", pl.ng, pl.wg,
-             pl.walker_ctas ? pl.walker_ctas : pl.nw, pl.ns, pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
+             pl.walker_ctas ? pl.walker_ctas : pl.nw, pl.isolate ? "(isolated)" : "", pl.ns,
+             pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
              any_cache ? "on" : "off");
     plan_text = buf;
     return CMC_OK;
@@ -225,6 +241,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     a.wg = pl.wg;
     a.ns = pl.ns;
     a.nw = pl.nw;
+    a.isolate_walkers = pl.isolate;
     a.group_bytes = pl.group_bytes;
     a.group_off = pl.group_off;
     a.slots_off = pl.slots_off;
@@ -447,7 +464,8 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "groups" && value >= 0 && value <= cmc::kMaxGroups) c->force_ng = uint32_t(value);
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
     else if (n == "method" && value >= -1 && value <= 1) c->force_method = int(value);
-    else if (n == "walkers" && value >= 0 && value <= 2) c->force_walkers = uint32_t(value);
+    else if (n == "walkers" && value >= 0 && value <= 4) c->force_walkers = uint32_t(value);
+    else if (n == "isolate_walkers" && value >= -1 && value <= 1) c->force_isolate = int(value);
     else if (n == "walker_ctas" && value >= -1 && value < c->sms) c->force_walker_ctas = int(value);
     else if (n == "slots_per_group" && value >= 0 && value <= 32)
         c->max_slots_per_group = value ? uint32_t(value) : 8u;

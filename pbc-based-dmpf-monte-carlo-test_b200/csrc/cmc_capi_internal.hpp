@@ -14,6 +14,7 @@ namespace cmc {
 struct Plan {
     uint32_t ng = 0, wg = 0, ns = 0, nw = 1;
     uint32_t walker_ctas = 0;  // > 0: split engine with this many walker CTAs
+    uint32_t isolate = 0;      // walker warps alone on SM sub-partition 3
     bool slots_smem = true;
     uint32_t slot_stride = 0, bins_bytes = 0, group_bytes = 0;
     uint32_t group_off = 0, slots_off = 0, smem_bytes = 0, threads = 0, ctas = 0;
@@ -48,6 +49,7 @@ struct Ctx {
     uint32_t force_wg = 0, force_ng = 0, force_global_slots = 0, force_walkers = 0;
     uint32_t max_slots_per_group = 8;
     int force_walker_ctas = -1;  // -1 auto, 0 in-SM walker, N split engine
+    int force_isolate = -1;      // -1 auto, 0 contiguous warp roles, 1 isolated walkers
     int force_method = -1;  // -1 auto, 0 direct, 1 cache
     uint32_t spin_limit = 1u << 26;
 

@@ -229,9 +229,9 @@ __device__ __forceinline__ void build_map_cache(const Job& J, GroupHeader* gh,
 }
 
 template <typename MapT, typename BinT, bool WIDE, bool SPLIT>
-__device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaShared* cs, uint32_t g) {
+__device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaShared* cs, uint32_t g,
+                                         uint32_t gt) {
     const uint32_t gthreads = a.wg * 32;
-    const uint32_t gt = threadIdx.x - g * gthreads;
     const uint32_t lane = threadIdx.x & 31;
     const Lanes L{lane * 4, lane * 4 + 128};
     char* gbase = smem + a.group_off + g * a.group_bytes;
@@ -744,7 +744,9 @@ __global__ void __launch_bounds__(512, 1) cmc_engine_split(const EngineArgs a) {
     }
     __syncthreads();
     const uint32_t warp = threadIdx.x >> 5;
-    if (warp < a.ng * a.wg) producer<MapT, BinT, WIDE, true>(a, smem, nullptr, warp / a.wg);
+    if (warp < a.ng * a.wg)
+        producer<MapT, BinT, WIDE, true>(a, smem, nullptr, warp / a.wg,
+                                         threadIdx.x - (warp / a.wg) * a.wg * 32);
 }
 
 template <typename MapT, typename BinT, bool WIDE>
@@ -762,12 +764,26 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
     if (threadIdx.x < kMaxSlots) cs->slot_state[threadIdx.x] = kSlotFree;
     if (threadIdx.x == 0) cs->groups_done = 0;
     __syncthreads();
-    const uint32_t warp = threadIdx.x >> 5;
-    if (warp < a.ng * a.wg) producer<MapT, BinT, WIDE, false>(a, smem, cs, warp / a.wg);
-    else if (warp < a.ng * a.wg + a.nw) {
-        const uint32_t wi = warp - a.ng * a.wg;
-        if (a.gslots) walker<MapT, BinT, false>(a, cs, wi);
-        else walker<MapT, BinT, true>(a, cs, wi);
+    // Warp roles.  Warp w issues from SM sub-partition w % 4.  With
+    // isolate_walkers the walker warps take ids 3, 7, 11, 15 -- sub-partition
+    // 3 alone -- so the latency-bound walks never wait for issue slots behind
+    // the throughput-bound AES warps, which fill sub-partitions 0..2.
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t producer_idx = 0xffffffffu, walker_idx = 0xffffffffu;
+    if (a.isolate_walkers) {
+        if ((warp & 3) == 3) walker_idx = warp >> 2;
+        else producer_idx = warp - (warp >> 2);
+    } else if (warp < a.ng * a.wg) {
+        producer_idx = warp;
+    } else {
+        walker_idx = warp - a.ng * a.wg;
+    }
+    if (producer_idx < a.ng * a.wg) {
+        const uint32_t g = producer_idx / a.wg;
+        producer<MapT, BinT, WIDE, false>(a, smem, cs, g, (producer_idx % a.wg) * 32 + lane);
+    } else if (walker_idx < a.nw) {
+        if (a.gslots) walker<MapT, BinT, false>(a, cs, walker_idx);
+        else walker<MapT, BinT, true>(a, cs, walker_idx);
     }
 }
 

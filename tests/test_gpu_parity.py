@@ -16,12 +16,14 @@ ENGINE_VARIANTS = [
     {"warps_per_group": 4, "groups": 2},
     {"walker_ctas": 8},                        # split engine: 8 SMs walk, the rest build maps
     {"walker_ctas": 20, "warps_per_group": 8, "method": 0},
-    {"walkers": 2, "warps_per_group": 7},
+    {"walkers": 2, "warps_per_group": 7, "isolate_walkers": 0},
+    {"isolate_walkers": 1, "warps_per_group": 6, "walkers": 3},
+    {"isolate_walkers": 1, "warps_per_group": 1, "global_slots": 1},
 ]
 
 
 DEFAULTS = {"method": -1, "global_slots": 0, "warps_per_group": 0, "groups": 0, "walkers": 0,
-            "walker_ctas": -1}
+            "walker_ctas": -1, "isolate_walkers": -1}
 
 
 def apply(ctx, opts):
@@ -79,7 +81,7 @@ def reference_cases(golden):
     return [r["name"] for r in golden["reference_runs"]]
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 6, 7])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 6, 7, 9, 10])
 def test_reference_runs(ctx, cmc, golden, variant):
     apply(ctx, ENGINE_VARIANTS[variant])
     for r in golden["reference_runs"]:
@@ -108,7 +110,7 @@ def random_shapes(n, seed):
 @pytest.mark.parametrize("shape", random_shapes(24, 7))
 def test_vs_oracle_random_shapes(ctx, cmc, oracle, shape):
     mode, im, pnum, ell, k, buckets, kick, seed, batch = shape
-    apply(ctx, ENGINE_VARIANTS[[0, 6, 7][seed % 3]])
+    apply(ctx, ENGINE_VARIANTS[[0, 6, 7, 9, 10][seed % 5]])
     p = cmc.parameters(mode, pnum, ell, k, buckets, kick, im)
     op = oracle.params(mode, pnum, ell, k, buckets, kick, im)
     count = 512 if pnum <= 100 else 96
