@@ -145,6 +145,7 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.isolate = pl.walker_ctas ? 0 : (force_isolate >= 0 ? uint32_t(force_isolate)
                                                           : (avg_probe_work >= 512 ? 1u : 0u));
     pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : (pl.isolate ? 2 : 1));
+    if (pl.isolate && !force_wg) pl.wg = any_cache ? 6 : 4;  // 12 producer warps in 2 or 3 groups
     if (pl.isolate && pl.nw > 4) pl.nw = 4;
     const uint32_t max_producer_warps = pl.isolate ? 12 : 16 - pl.nw;
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
