@@ -51,13 +51,23 @@ __device__ __forceinline__ uint32_t lds(uint32_t off) {
 struct Lanes {
     uint32_t lb0;  // lane*4
     uint32_t lb2;  // lane*4 + 128
+    // 256 held in a register (from a kernel argument): with it the offset of
+    // a top-byte lookup, (w >> 24) * 256 + lb0, is two multiply-adds on the
+    // FMA pipe instead of one byte permute on the ALU pipe, which the table
+    // lookups otherwise saturate.  0 selects the permute form everywhere.
+    uint32_t r256;
 };
+
+__device__ __forceinline__ uint32_t top_byte_off(const Lanes& L, uint32_t w) {
+    if (L.r256 == 0) return toff<3>(w, L.lb0);
+    return __umulhi(w, L.r256) * L.r256 + L.lb0;
+}
 
 // Column j of a full round: inputs s_j (byte 3), s_{j+1} (byte 2),
 // s_{j+2} (byte 1), s_{j+3} (byte 0); kr = rol8(round key word).
 __device__ __forceinline__ uint32_t column(const Lanes& L, uint32_t sa, uint32_t sb,
                                           uint32_t sc, uint32_t sd, uint32_t kr) {
-    const uint32_t a = lds(toff<3>(sa, L.lb0));
+    const uint32_t a = lds(top_byte_off(L, sa));
     const uint32_t b = lds(toff<2>(sb, L.lb0));
     const uint32_t c = lds(toff<1>(sc, L.lb2));
     const uint32_t d = lds(toff<0>(sd, L.lb2));

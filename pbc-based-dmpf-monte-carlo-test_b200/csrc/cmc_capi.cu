@@ -23,7 +23,8 @@ template <typename MapT, typename BinT, bool WIDE>
 __global__ void cmc_engine_split(const EngineArgs a);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
                                      uint32_t* out, uint32_t* count);
-__global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out);
+__global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out,
+                             uint32_t r256);
 
 namespace {
 
@@ -145,9 +146,9 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.isolate = pl.walker_ctas ? 0 : (force_isolate >= 0 ? uint32_t(force_isolate)
                                                           : (avg_probe_work >= 512 ? 1u : 0u));
     pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : (pl.isolate ? 2 : 1));
-    if (pl.isolate && !force_wg) pl.wg = any_cache ? 6 : 4;  // 12 producer warps in 2 or 3 groups
+    if (pl.isolate && !force_wg) pl.wg = any_cache ? 6 : 4;  // 2 or 3 groups of producers
     if (pl.isolate && pl.nw > 4) pl.nw = 4;
-    const uint32_t max_producer_warps = pl.isolate ? 12 : 16 - pl.nw;
+    const uint32_t max_producer_warps = 16 - pl.nw;
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
     uint32_t ng = std::min<uint32_t>(kMaxGroups, max_producer_warps / pl.wg);
     if (force_ng) ng = std::min(ng, force_ng);
@@ -181,10 +182,7 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.slots_off = pl.group_off + pl.ng * pl.group_bytes;
     pl.smem_bytes = pl.slots_off + (pl.slots_smem ? pl.ns * pl.slot_stride : 0);
     if (pl.isolate) {
-        const uint32_t P = pl.ng * pl.wg;
-        const uint32_t last_producer_warp = P ? (P - 1) + (P - 1) / 3 : 0;
-        const uint32_t last_walker_warp = pl.nw ? 4 * (pl.nw - 1) + 3 : 0;
-        pl.threads = (std::max(last_producer_warp, last_walker_warp) + 1) * 32;
+        pl.threads = 512;  // walker warps sit at ids 15, 11, ...; unused ids exit at once
     } else {
         pl.threads = (pl.ng * pl.wg + pl.nw) * 32;
     }
@@ -243,6 +241,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     a.ns = pl.ns;
     a.nw = pl.nw;
     a.isolate_walkers = pl.isolate;
+    a.r256 = fma_offsets ? 256u : 0u;
     a.group_bytes = pl.group_bytes;
     a.group_off = pl.group_off;
     a.slots_off = pl.slots_off;
@@ -320,7 +319,7 @@ int Ctx::init(int dev) {
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kat_smem),
                    "selftest attribute")))
         return rc;
-    cmc_selftest<<<1, 32, kat_smem, stream>>>(d_t0, d_t0 + 256, d_t0 + 300);
+    cmc_selftest<<<1, 32, kat_smem, stream>>>(d_t0, d_t0 + 256, d_t0 + 300, 256u);
     if ((rc = cuda(cudaGetLastError(), "selftest launch"))) return rc;
     uint32_t bad[32];
     if ((rc = cuda(cudaMemcpyAsync(bad, d_t0 + 300, sizeof bad, cudaMemcpyDeviceToHost, stream),
@@ -467,6 +466,7 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "method" && value >= -1 && value <= 1) c->force_method = int(value);
     else if (n == "walkers" && value >= 0 && value <= 4) c->force_walkers = uint32_t(value);
     else if (n == "isolate_walkers" && value >= -1 && value <= 1) c->force_isolate = int(value);
+    else if (n == "fma_offsets" && (value == 0 || value == 1)) c->fma_offsets = uint32_t(value);
     else if (n == "walker_ctas" && value >= -1 && value < c->sms) c->force_walker_ctas = int(value);
     else if (n == "slots_per_group" && value >= 0 && value <= 32)
         c->max_slots_per_group = value ? uint32_t(value) : 8u;

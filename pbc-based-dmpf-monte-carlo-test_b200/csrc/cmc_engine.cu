@@ -233,7 +233,7 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
                                          uint32_t gt) {
     const uint32_t gthreads = a.wg * 32;
     const uint32_t lane = threadIdx.x & 31;
-    const Lanes L{lane * 4, lane * 4 + 128};
+    const Lanes L{lane * 4, lane * 4 + 128, a.r256};
     char* gbase = smem + a.group_off + g * a.group_bytes;
     GroupHeader* gh = reinterpret_cast<GroupHeader*>(gbase);
     uint16_t* cache = reinterpret_cast<uint16_t*>(gbase + sizeof(GroupHeader));
@@ -765,14 +765,22 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
     if (threadIdx.x == 0) cs->groups_done = 0;
     __syncthreads();
     // Warp roles.  Warp w issues from SM sub-partition w % 4.  With
-    // isolate_walkers the walker warps take ids 3, 7, 11, 15 -- sub-partition
-    // 3 alone -- so the latency-bound walks never wait for issue slots behind
-    // the throughput-bound AES warps, which fill sub-partitions 0..2.
+    // isolate_walkers the nw walker warps take ids 15, 11, 7, 3 -- all on
+    // sub-partition 3, which then hosts at most 4 - nw producer warps -- so
+    // the latency-bound walks compete with few throughput-bound AES warps for
+    // issue slots.  Producers take the remaining ids in order.
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t producer_idx = 0xffffffffu, walker_idx = 0xffffffffu;
     if (a.isolate_walkers) {
-        if ((warp & 3) == 3) walker_idx = warp >> 2;
-        else producer_idx = warp - (warp >> 2);
+        const bool walker_warp = (warp & 3) == 3 && (15 - warp) / 4 < a.nw;
+        if (walker_warp) {
+            walker_idx = (15 - warp) / 4;
+        } else {
+            // walker warps below this one: ids 15, 11, ... that are < warp
+            uint32_t below = 0;
+            for (uint32_t i = 0; i < a.nw; ++i) below += (15 - 4 * i) < warp;
+            producer_idx = warp - below;
+        }
     } else if (warp < a.ng * a.wg) {
         producer_idx = warp;
     } else {
@@ -832,7 +840,8 @@ __global__ void __launch_bounds__(1024) cmc_compact_failures(const uint32_t* __r
 // Device self-test: the FIPS-197 AES-128 vector on every lane through the
 // shared-memory table, and the 124-lookup PRP round function against the
 // full encryption for pseudo-random keys, rounds and inputs.
-__global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out) {
+__global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out,
+                             uint32_t r256) {
     char* smem = cmc_dyn_smem;
     uint32_t* tw = reinterpret_cast<uint32_t*>(smem);
     for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) {
@@ -841,7 +850,8 @@ __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32
     }
     __syncthreads();
     const uint32_t lane = threadIdx.x & 31;
-    const Lanes L{lane * 4, lane * 4 + 128};
+    const Lanes L{lane * 4, lane * 4 + 128, 0};       // byte-permute offsets
+    const Lanes LF{lane * 4, lane * 4 + 128, r256};   // FMA-pipe top-byte offsets
     uint32_t c[4];
     encrypt_full(L, fips_rk, 0x00112233u, 0x44556677u, 0x8899aabbu, 0xccddeeffu, c);
     uint32_t bad = 0;
@@ -866,6 +876,11 @@ __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32
         uint32_t full[4];
         encrypt_full(L, rk, 0x43455350u, r, h, R, full);
         if ((prp_f(L, key, rc, R) & 0xffffu) != (full[3] & 0xffffu)) bad |= 4;
+        if ((prp_f(LF, key, rc, R) & 0xffffu) != (full[3] & 0xffffu)) bad |= 8;
+        uint32_t full2[4];
+        encrypt_full(LF, rk, 0x43455350u, r, h, R, full2);
+        for (int j = 0; j < 4; ++j)
+            if (full2[j] != full[j]) bad |= 16;
     }
     out[threadIdx.x] = bad;
 }

@@ -65,7 +65,8 @@ struct EngineArgs {
     uint32_t bins_bytes;                // map starts this far into a slot
     uint32_t ng, wg, ns;                // groups, warps per group, slots
     uint32_t nw;                        // walker warps (slot s -> walker s % nw)
-    uint32_t isolate_walkers;           // walkers on warps 3, 7, 11, 15 only
+    uint32_t isolate_walkers;           // walkers on warps 15, 11, 7, 3 (sub-partition 3)
+    uint32_t r256;                      // 256 to use the FMA-pipe lookup offsets, 0 not to
     // split engine: CTAs [0, producer_ctas) produce maps, the rest walk; slot s
     // is walked by thread s of the walker CTAs; headers in global memory
     GSlotHeader* ghdr;
