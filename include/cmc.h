@@ -99,9 +99,7 @@ int cmc_check(cmc_ctx* ctx);
  * on SM sub-partition 3, producers on 0..2), "slots_per_group" (cap on shared-memory slots per
  * group, default 8), "walker_ctas" (-1 auto, 0 walks inside each CTA, N > 0
  * dedicates N CTAs -- one per SM -- to walks over global slots while the
- * others only build maps), "fma_offsets" (1 default / 0: compute the
- * offsets of top-byte table lookups on the FMA pipe or with byte permutes),
- * "spin_limit" (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown
+ * others only build maps), "spin_limit" (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown
  * name or a value out of range. */
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
 

@@ -145,8 +145,10 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     avg_probe_work = work > 0 ? avg_probe_work / work : 0;
     pl.isolate = pl.walker_ctas ? 0 : (force_isolate >= 0 ? uint32_t(force_isolate)
                                                           : (avg_probe_work >= 512 ? 1u : 0u));
-    pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : (pl.isolate ? 2 : 1));
-    if (pl.isolate && !force_wg) pl.wg = any_cache ? 6 : 4;  // 2 or 3 groups of producers
+    pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : 1);
+    // measured best with isolated walkers: 2 groups of 7 producer warps (12
+    // on sub-partitions 0..2, 2 beside the walker on sub-partition 3)
+    if (pl.isolate && !force_wg) pl.wg = any_cache ? 7 : 4;
     if (pl.isolate && pl.nw > 4) pl.nw = 4;
     const uint32_t max_producer_warps = 16 - pl.nw;
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
@@ -241,7 +243,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     a.ns = pl.ns;
     a.nw = pl.nw;
     a.isolate_walkers = pl.isolate;
-    a.r256 = fma_offsets ? 256u : 0u;
+    a.r256 = 256u;
     a.group_bytes = pl.group_bytes;
     a.group_off = pl.group_off;
     a.slots_off = pl.slots_off;
@@ -466,7 +468,6 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "method" && value >= -1 && value <= 1) c->force_method = int(value);
     else if (n == "walkers" && value >= 0 && value <= 4) c->force_walkers = uint32_t(value);
     else if (n == "isolate_walkers" && value >= -1 && value <= 1) c->force_isolate = int(value);
-    else if (n == "fma_offsets" && (value == 0 || value == 1)) c->fma_offsets = uint32_t(value);
     else if (n == "walker_ctas" && value >= -1 && value < c->sms) c->force_walker_ctas = int(value);
     else if (n == "slots_per_group" && value >= 0 && value <= 32)
         c->max_slots_per_group = value ? uint32_t(value) : 8u;

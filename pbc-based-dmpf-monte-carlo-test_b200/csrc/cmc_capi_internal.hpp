@@ -50,7 +50,6 @@ struct Ctx {
     uint32_t max_slots_per_group = 8;
     int force_walker_ctas = -1;  // -1 auto, 0 in-SM walker, N split engine
     int force_isolate = -1;      // -1 auto, 0 contiguous warp roles, 1 isolated walkers
-    uint32_t fma_offsets = 1;    // top-byte lookup offsets on the FMA pipe
     int force_method = -1;  // -1 auto, 0 direct, 1 cache
     uint32_t spin_limit = 1u << 26;
 

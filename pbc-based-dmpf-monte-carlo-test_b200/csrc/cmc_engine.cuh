@@ -66,7 +66,7 @@ struct EngineArgs {
     uint32_t ng, wg, ns;                // groups, warps per group, slots
     uint32_t nw;                        // walker warps (slot s -> walker s % nw)
     uint32_t isolate_walkers;           // walkers on warps 15, 11, 7, 3 (sub-partition 3)
-    uint32_t r256;                      // 256 to use the FMA-pipe lookup offsets, 0 not to
+    uint32_t r256;                      // the constant 256, kept opaque to the compiler
     // split engine: CTAs [0, producer_ctas) produce maps, the rest walk; slot s
     // is walked by thread s of the walker CTAs; headers in global memory
     GSlotHeader* ghdr;
