@@ -146,9 +146,9 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.isolate = pl.walker_ctas ? 0 : (force_isolate >= 0 ? uint32_t(force_isolate)
                                                           : (avg_probe_work >= 512 ? 1u : 0u));
     pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : 1);
-    // measured best with isolated walkers: 2 groups of 7 producer warps (12
-    // on sub-partitions 0..2, 2 beside the walker on sub-partition 3)
-    if (pl.isolate && !force_wg) pl.wg = any_cache ? 7 : 4;
+    // measured best with isolated walkers: 2 groups of 6 producer warps on
+    // sub-partitions 0..2 (2 x 7, adding two beside the walker, is within 3%)
+    if (pl.isolate && !force_wg) pl.wg = any_cache ? 6 : 4;
     if (pl.isolate && pl.nw > 4) pl.nw = 4;
     const uint32_t max_producer_warps = 16 - pl.nw;
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
