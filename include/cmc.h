@@ -103,6 +103,25 @@ int cmc_check(cmc_ctx* ctx);
  * name or a value out of range. */
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
 
+/* No counterpart in the reference.  The Launch seam for callers that cannot
+ * let this library allocate device memory -- e.g. a process whose device
+ * memory is owned by another framework's caching allocator, or a service loop
+ * that must not pay cudaMalloc/cudaFree's device-wide synchronisation.  Same
+ * result as cmc_launch_device, on the current device, with no context and no
+ * allocation: the working memory is a fixed file-scope device array (about
+ * 129 KiB per GPU, held until the process exits).  Limits: count is 1..2^20
+ * trials per call, and parameter sets whose walk slots do not fit in shared
+ * memory are rejected (CMC_EINVAL).  d_batch_key, d_out_offsets (capacity
+ * count) and d_out_nfailed are device pointers; work is queued on `stream`.
+ * The first call on a device sets up that device (symbol addresses, a 1 KiB
+ * table upload), so it should come before any stream capture.  All calls on a
+ * device share the working memory: calls that overlap on the GPU race, so order
+ * them (e.g. one stream).  If a bounded device wait gives up, *d_out_nfailed is
+ * set to 0xffffffff.  Errors: cmc_last_error(NULL). */
+int cmc_launch_static(const cmc_params* params, const uint32_t* d_batch_key, uint32_t first,
+                      uint32_t count, uint32_t* d_out_offsets, uint32_t* d_out_nfailed,
+                      void* stream);
+
 /* Queue this context's host-buffer launches (cmc_launch) on `stream`
  * (cudaStream_t; NULL restores the context's own stream). */
 int cmc_set_stream(cmc_ctx* ctx, void* stream);

@@ -36,7 +36,7 @@ EXPORTS = (
     "cmc_derive_params", "cmc_batch_key", "cmc_host_aes128", "cmc_init", "cmc_destroy",
     "cmc_last_error", "cmc_launch", "cmc_launch_device", "cmc_check",
     "cmc_last_kernel_count", "cmc_last_plan", "cmc_set_option",
-    "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats",
+    "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats", "cmc_launch_static",
 )
 
 
@@ -110,6 +110,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.cmc_last_engine_ms.restype = ctypes.c_double
     lib.cmc_last_stats.argtypes = [vp, P(u64)]
     lib.cmc_last_stats.restype = ctypes.c_int
+    lib.cmc_launch_static.argtypes = [P(Params), vp, u32, u32, vp, vp, vp]
+    lib.cmc_launch_static.restype = ctypes.c_int
     lib.cmc_last_plan.argtypes = [vp]
     lib.cmc_last_plan.restype = ctypes.c_char_p
     if path is None:
@@ -225,6 +227,21 @@ class Context:
     @property
     def last_kernel_count(self) -> int:
         return self.lib.cmc_last_kernel_count(self.handle)
+
+
+STATIC_MAX_TRIALS = 1 << 20
+
+
+def launch_static(params: Params, d_key: int, first: int, count: int, d_offsets: int,
+                  d_nfailed: int, stream: int = 0) -> None:
+    """cmc_launch_static: the Launch seam without any device allocation by the
+    library (device pointers in and out, current device, asynchronous)."""
+    lib = load_library()
+    rc = lib.cmc_launch_static(ctypes.byref(params), ctypes.c_void_p(d_key), first, count,
+                               ctypes.c_void_p(d_offsets), ctypes.c_void_p(d_nfailed),
+                               ctypes.c_void_p(stream))
+    if rc:
+        raise CmcError(rc, lib.cmc_last_error(None).decode())
 
 
 def process_batch(ctx: Context, params: Params, seed: int, batch_id: int, batch_trials: int,

@@ -37,6 +37,8 @@ uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
 
+void set_thread_error(const std::string& message) { g_thread_error = message; }
+
 int Ctx::fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
