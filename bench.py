@@ -234,6 +234,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--trials", type=int, default=1 << 20,
+                    help="trials per step (default one batch, 2^20); smaller for profiling")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -256,7 +258,7 @@ def main():
     w = WORKLOAD
     p = cmc.parameters(w["mode"], w["pnum"], w["ell_i"], w["k"], w["buckets"], w["kick"],
                        w["input_mode"])
-    n = 1 << w["bt"]
+    n = min(args.trials, 1 << w["bt"])
     # a dedicated stream: the legacy default stream's handle is NULL, which the
     # C ABI reads as "the context's own stream"
     stream = torch.cuda.Stream()
