@@ -225,6 +225,75 @@ def run_reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------ sweep workload --
+
+def sweep_sets(n_sets: int = 64, draw_seed: int = 3):
+    """The mixed sweep: n_sets parameter sets drawn with draw_seed.  t is
+    log-uniform over 16..4096, B = ceil(r t) with r in {1.25, 1.35, 1.5}, k in
+    {2, 3, 4}, max kicks in {100, 500}, N = 2^24 (ell_i 24), BGH25, affine
+    inputs.  Set i is its own experiment with seed draw_seed*1000 + i."""
+    import numpy as np
+    rng = np.random.default_rng(draw_seed)
+    sets = []
+    for i in range(n_sets):
+        t = int(round(math.exp(rng.uniform(math.log(16), math.log(4096)))))
+        r = float(rng.choice([1.25, 1.35, 1.5]))
+        k = int(rng.choice([2, 3, 4]))
+        kick = int(rng.choice([100, 500]))
+        sets.append(dict(mode="bgh25", pnum=max(t, 3), ell_i=24, k=k, buckets=math.ceil(r * t),
+                         kick=kick, input_mode="affine", seed=draw_seed * 1000 + i))
+    return sets
+
+
+def run_sweep_workload(args):
+    """Plain (one launch per parameter set) vs batched (all sets in one
+    persistent launch) on the mixed sweep; both must give identical failures."""
+    import torch
+    cmc = load_pkg()
+    ctx = cmc.Context(0)
+    sets = sweep_sets()
+    n = args.sweep_trials
+    params = [cmc.parameters(s["mode"], s["pnum"], s["ell_i"], s["k"], s["buckets"], s["kick"],
+                             s["input_mode"]) for s in sets]
+    jobs = [(p, s["seed"], 0, 0, n) for p, s in zip(params, sets)]
+    total = n * len(sets)
+
+    def plain():
+        fails = []
+        for p, s in zip(params, sets):
+            fails.append(ctx.launch(p, cmc.batch_key(s["seed"], 0), 0, n))
+        return fails
+
+    def batched():
+        counts, per_job = ctx.run_jobs(jobs)
+        return [per_job[i] for i in range(len(jobs))]
+
+    # warm-up (also the correctness check)
+    ref = plain()
+    got = batched()
+    same = ref == got
+    torch.cuda.synchronize()
+    t0 = time.perf_counter(); plain(); t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter(); batched(); t_batched = time.perf_counter() - t0
+    choice = ctx.autotune(jobs, sample_div=64)
+    batched()
+    t0 = time.perf_counter(); tuned = batched(); t_tuned = time.perf_counter() - t0
+    same = same and tuned == ref
+    avg_blocks = sum(algorithmic_blocks(p) for p in params) / len(params)
+    line = {
+        "metric": "sweep trials/s (64 mixed parameter sets, bit-exact failures)",
+        "workload": f"sweep: 64 sets drawn with seed 3, {n} trials each",
+        "plain_trials_per_s": total / t_plain, "batched_trials_per_s": total / t_batched,
+        "batched_tuned_trials_per_s": total / t_tuned,
+        "speedup_batched_vs_plain": t_plain / t_tuned,
+        "identical_failures": same, "failures": sum(len(f) for f in ref),
+        "mean_aes_blocks_per_trial": avg_blocks, "tuned_plan": choice,
+        "timing": "host wall clock around synchronous C-ABI calls (cmc_launch / cmc_run_jobs)",
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 # ------------------------------------------------------------------ our arm --
 
 def main():
@@ -236,6 +305,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--trials", type=int, default=1 << 20,
                     help="trials per step (default one batch, 2^20); smaller for profiling")
+    ap.add_argument("--workload", choices=["config2", "sweep"], default="config2")
+    ap.add_argument("--sweep-trials", type=int, default=1 << 16,
+                    help="trials per parameter set for --workload sweep")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -244,6 +316,10 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.workload == "sweep":
+        if rank == 0:
+            run_sweep_workload(args)
         return
 
     import torch

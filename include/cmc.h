@@ -91,6 +91,35 @@ int cmc_launch_device(cmc_ctx* ctx, const cmc_params* params, const uint32_t* d_
                       uint32_t* d_out_nfailed, void* stream);
 int cmc_check(cmc_ctx* ctx);
 
+/* One entry of a batched launch: a parameter set and a run of trials of one
+ * batch of its experiment (key = cmc_batch_key(seed, batch)). */
+typedef struct cmc_job {
+    cmc_params params;
+    uint64_t seed;
+    uint64_t batch;
+    uint32_t first;  /* first within-batch offset */
+    uint32_t count;  /* trials */
+} cmc_job;
+
+/* Batched form (no counterpart in the reference, which runs one parameter set
+ * per process): all jobs in ONE persistent engine launch, heavy jobs first so
+ * uneven table sizes balance across SMs.  out_failed[j] receives the number of
+ * failing trials of job j.  If out_offsets is not NULL, the failing offsets are
+ * written job by job in ascending order, out_jobs[i] (if not NULL) naming the
+ * job of out_offsets[i]; cap is their capacity and *out_total the number of
+ * failures (when it exceeds cap, only the counts are complete).  Total trials
+ * per call must be below 2^32.  Synchronous. */
+int cmc_run_jobs(cmc_ctx* ctx, const cmc_job* jobs, uint32_t njobs, uint64_t* out_failed,
+                 uint32_t* out_offsets, uint32_t* out_jobs, uint64_t cap, uint64_t* out_total);
+
+/* Autotuner: times candidate plans (warps per table, walker isolation, map
+ * method) on a sample of every job (first count/sample_div trials, at least
+ * one), keeps the fastest for this mix of parameter sets, and applies it to
+ * later cmc_run_jobs calls with the same mix.  *out_choice (may be NULL)
+ * receives a description of the chosen plan. */
+int cmc_autotune(cmc_ctx* ctx, const cmc_job* jobs, uint32_t njobs, uint32_t sample_div,
+                 const char** out_choice);
+
 /* Tuning knobs of the launch planner; value 0 (or -1 for "method") restores
  * the automatic choice.  Names: "warps_per_group" (1..15), "groups" (1..14),
  * "global_slots" (0/1: keep walk slots in global memory), "method"

@@ -37,6 +37,7 @@ EXPORTS = (
     "cmc_last_error", "cmc_launch", "cmc_launch_device", "cmc_check",
     "cmc_last_kernel_count", "cmc_last_plan", "cmc_set_option",
     "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats", "cmc_launch_static",
+    "cmc_run_jobs", "cmc_autotune",
 )
 
 
@@ -66,6 +67,18 @@ class Params(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Job(ctypes.Structure):
+    """cmc_job: one parameter set and a run of trials of one batch."""
+
+    _fields_ = [
+        ("params", Params),
+        ("seed", ctypes.c_uint64),
+        ("batch", ctypes.c_uint64),
+        ("first", ctypes.c_uint32),
+        ("count", ctypes.c_uint32),
+    ]
 
 
 _lib = None
@@ -112,6 +125,10 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.cmc_last_stats.restype = ctypes.c_int
     lib.cmc_launch_static.argtypes = [P(Params), vp, u32, u32, vp, vp, vp]
     lib.cmc_launch_static.restype = ctypes.c_int
+    lib.cmc_run_jobs.argtypes = [vp, P(Job), u32, P(u64), P(u32), P(u32), u64, P(u64)]
+    lib.cmc_run_jobs.restype = ctypes.c_int
+    lib.cmc_autotune.argtypes = [vp, P(Job), u32, u32, P(ctypes.c_char_p)]
+    lib.cmc_autotune.restype = ctypes.c_int
     lib.cmc_last_plan.argtypes = [vp]
     lib.cmc_last_plan.restype = ctypes.c_char_p
     if path is None:
@@ -200,6 +217,39 @@ class Context:
         rc = self.lib.cmc_check(self.handle)
         if rc:
             self._raise(rc)
+
+    def run_jobs(self, jobs: list[tuple], cap: int | None = None):
+        """Batched launch.  jobs: (params, seed, batch, first, count) tuples.
+        Returns (failed counts per job, {job index: sorted failing offsets})."""
+        n = len(jobs)
+        arr = (Job * n)()
+        total_trials = 0
+        for i, (p, seed, batch, first, count) in enumerate(jobs):
+            arr[i] = Job(p, seed, batch, first, count)
+            total_trials += count
+        cap = total_trials if cap is None else cap
+        failed = (ctypes.c_uint64 * n)()
+        offs = (ctypes.c_uint32 * max(cap, 1))()
+        which = (ctypes.c_uint32 * max(cap, 1))()
+        total = ctypes.c_uint64()
+        rc = self.lib.cmc_run_jobs(self.handle, arr, n, failed, offs, which, cap, ctypes.byref(total))
+        if rc:
+            self._raise(rc)
+        per_job: dict[int, list[int]] = {i: [] for i in range(n)}
+        for i in range(min(total.value, cap)):
+            per_job[which[i]].append(offs[i])
+        return list(failed), per_job
+
+    def autotune(self, jobs: list[tuple], sample_div: int = 64) -> str:
+        n = len(jobs)
+        arr = (Job * n)()
+        for i, (p, seed, batch, first, count) in enumerate(jobs):
+            arr[i] = Job(p, seed, batch, first, count)
+        choice = ctypes.c_char_p()
+        rc = self.lib.cmc_autotune(self.handle, arr, n, sample_div, ctypes.byref(choice))
+        if rc:
+            self._raise(rc)
+        return choice.value.decode()
 
     def set_option(self, name: str, value: int) -> None:
         rc = self.lib.cmc_set_option(self.handle, name.encode(), value)

@@ -22,7 +22,7 @@ __global__ void cmc_engine(const EngineArgs a);
 template <typename MapT, typename BinT, bool WIDE>
 __global__ void cmc_engine_split(const EngineArgs a);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
-                                     uint32_t* out, uint32_t* count);
+                                     uint32_t* out, uint32_t* count, uint64_t cap);
 __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out,
                              uint32_t r256);
 
@@ -206,8 +206,8 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
 // Queue one engine launch over `jobs` (already on the device in d_jobs) and
 // the compaction of its failure bitmap.
 int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint32_t value_base,
-             uint32_t* d_out, uint32_t* d_count, unsigned long long* job_failed,
-             unsigned long long* job_done) {
+             uint32_t* d_out, uint32_t* d_count, uint64_t out_cap_now,
+             unsigned long long* job_failed, unsigned long long* job_done) {
     Plan pl;
     int rc = plan(jobs, pl);
     if (rc) return rc;
@@ -275,7 +275,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     if ((rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
     kernels = 1;
     if (d_out) {
-        cmc_compact_failures<<<1, 1024, 0, st>>>(d_bits, total, value_base, d_out, d_count);
+        cmc_compact_failures<<<1, 1024, 0, st>>>(d_bits, total, value_base, d_out, d_count, out_cap_now);
         if ((rc = cuda(cudaGetLastError(), "compaction launch"))) return rc;
         kernels = 2;
     }
@@ -344,6 +344,7 @@ Ctx::~Ctx() {
     cudaFree(d_out);
     cudaFree(d_slots);
     cudaFree(d_ghdr);
+    cudaFree(d_job_failed);
     cudaFree(d_key);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
@@ -373,7 +374,7 @@ int Ctx::launch_host(const cmc_params& p, const uint32_t key[44], uint32_t first
     std::memcpy(jobs[0].batch_rk, key, 44 * 4);
     if ((rc = upload_jobs(jobs, st))) return rc;
     if ((rc = grow(d_out, out_cap, size_t(count) + 1, "failure list"))) return rc;
-    if ((rc = run(jobs, count, st, first, d_out, d_out + count, nullptr, nullptr))) return rc;
+    if ((rc = run(jobs, count, st, first, d_out, d_out + count, count, nullptr, nullptr))) return rc;
     uint32_t nf = 0;
     if ((rc = cuda(cudaMemcpyAsync(&nf, d_out + count, 4, cudaMemcpyDeviceToHost, st), "read count")))
         return rc;
@@ -402,7 +403,199 @@ int Ctx::launch_device(const cmc_params& p, const uint32_t* d_key_in, uint32_t f
     if ((rc = cuda(cudaMemcpyAsync(d_jobs[0].batch_rk, d_key_in, 44 * 4, cudaMemcpyDeviceToDevice, st),
                    "copy batch key")))
         return rc;
-    return run(jobs, count, st, first, d_offsets, d_nfailed, nullptr, nullptr);
+    return run(jobs, count, st, first, d_offsets, d_nfailed, count, nullptr, nullptr);
+}
+
+// Estimated AES-block cost of one trial of a job (map build + seeds), used to
+// order a batch heaviest first.
+static double job_cost(const Job& j) {
+    const double c = std::ldexp(1.0, 2 * int(j.half_bits)) / double(j.domain);
+    const double direct = double(j.pnum) * j.k * 8.0 * c;
+    const double cache = 8.0 * std::ldexp(1.0, int(j.half_bits)) + direct / 64.0;
+    return 2.0 + (j.method == kMethodCache ? cache : direct) + 0.1 * j.pnum;
+}
+
+std::string Ctx::mix_key(const cmc_job* in, uint32_t n) const {
+    std::vector<std::string> parts;
+    for (uint32_t i = 0; i < n; ++i) {
+        const cmc_params& p = in[i].params;
+        char b[96];
+        snprintf(b, sizeof b, "%u/%u/%u/%u/%u/%llu", p.mode, p.pnum, p.k, p.buckets, p.half_bits,
+                 (unsigned long long)p.domain);
+        parts.push_back(b);
+    }
+    std::sort(parts.begin(), parts.end());
+    parts.erase(std::unique(parts.begin(), parts.end()), parts.end());
+    std::string key;
+    for (auto& x : parts) key += x + ";";
+    return key;
+}
+
+int Ctx::prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::vector<Job>& out,
+                      std::vector<uint32_t>& order, uint64_t& total) {
+    if (!in || n == 0) return fail(CMC_EINVAL, "no jobs");
+    std::vector<Job> tmp(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t count = in[i].count;
+        if (sample_div > 1) count = std::max<uint32_t>(1, count / sample_div);
+        if (count == 0) return fail(CMC_EINVAL, "job %u has no trials", i);
+        if (uint64_t(in[i].first) + count > 0x100000000ULL)
+            return fail(CMC_EINVAL, "job %u: offset range overflows", i);
+        int rc = make_job(in[i].params, in[i].first, count, 0, tmp[i]);
+        if (rc) return rc;
+        batch_key(in[i].seed, in[i].batch, tmp[i].batch_rk);
+        tmp[i].user = i;
+    }
+    order.resize(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return job_cost(tmp[a]) > job_cost(tmp[b]); });
+    out.resize(n);
+    total = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        out[i] = tmp[order[i]];
+        out[i].trial_base = total;
+        total += out[i].count;
+    }
+    if (total >= 0xffffffffULL) return fail(CMC_EINVAL, "more than 2^32 - 1 trials in one batched call");
+    return CMC_OK;
+}
+
+namespace {
+
+// Apply a tuned plan for the duration of one call.
+struct ScopedPlan {
+    Ctx& c;
+    uint32_t wg;
+    int isolate, method;
+    ScopedPlan(Ctx& ctx, const TunedPlan* t) : c(ctx), wg(ctx.force_wg), isolate(ctx.force_isolate),
+                                               method(ctx.force_method) {
+        if (t) {
+            c.force_wg = t->wg;
+            c.force_isolate = t->isolate;
+            c.force_method = t->method;
+        }
+    }
+    ~ScopedPlan() {
+        c.force_wg = wg;
+        c.force_isolate = isolate;
+        c.force_method = method;
+    }
+};
+
+}  // namespace
+
+int Ctx::run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t* out_offsets,
+                  uint32_t* out_jobs, uint64_t cap, uint64_t* out_total) {
+    kernels = 0;
+    if (!out_failed) return fail(CMC_EINVAL, "null out_failed");
+    int rc = cuda(cudaSetDevice(device), "cudaSetDevice");
+    if (rc) return rc;
+    const auto it = tuned.find(mix_key(in, n));
+    ScopedPlan scoped(*this, it == tuned.end() ? nullptr : &it->second);
+    std::vector<Job> jobs;
+    std::vector<uint32_t> order;
+    uint64_t total = 0;
+    if ((rc = prepare_jobs(in, n, 0, jobs, order, total))) return rc;
+    cudaStream_t st = user_stream ? user_stream : stream;
+    if ((rc = upload_jobs(jobs, st))) return rc;
+    if ((rc = grow(d_job_failed, job_failed_cap, n, "job counters"))) return rc;
+    if ((rc = cuda(cudaMemsetAsync(d_job_failed, 0, n * sizeof(unsigned long long), st), "memset counters")))
+        return rc;
+    const uint64_t dev_cap = out_offsets ? std::min<uint64_t>(cap, total) : 0;
+    if ((rc = grow(d_out, out_cap, size_t(dev_cap) + 1, "failure list"))) return rc;
+    if ((rc = run(jobs, total, st, 0, d_out, d_out + dev_cap, dev_cap, d_job_failed, nullptr))) return rc;
+    std::vector<unsigned long long> failed(n);
+    uint32_t nf = 0;
+    if ((rc = cuda(cudaMemcpyAsync(failed.data(), d_job_failed, n * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, st), "read counters")))
+        return rc;
+    if ((rc = cuda(cudaMemcpyAsync(&nf, d_out + dev_cap, 4, cudaMemcpyDeviceToHost, st), "read count")))
+        return rc;
+    if ((rc = cuda(cudaStreamSynchronize(st), "batched sync"))) return rc;
+    if ((rc = check_ctrl())) return rc;
+    uint64_t sum = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        out_failed[order[i]] = failed[i];
+        sum += failed[i];
+    }
+    if (sum != nf) return fail(CMC_ERANGE, "per-job failure counts disagree with the bitmap");
+    if (out_total) *out_total = nf;
+    if (out_offsets && nf) {
+        const uint64_t m = std::min<uint64_t>(nf, dev_cap);
+        std::vector<uint32_t> g(m);
+        if ((rc = cuda(cudaMemcpy(g.data(), d_out, m * 4, cudaMemcpyDeviceToHost), "read failures"))) return rc;
+        // global index -> (original job, offset); global order is job-major in
+        // the heavy-first order, so regroup by the caller's job order
+        std::vector<std::pair<uint32_t, uint32_t>> pairs(m);
+        for (uint64_t i = 0; i < m; ++i) {
+            uint32_t lo = 0, hi = n;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) / 2;
+                if (jobs[mid].trial_base <= g[i]) lo = mid; else hi = mid;
+            }
+            pairs[i] = {order[lo], jobs[lo].first + uint32_t(g[i] - jobs[lo].trial_base)};
+        }
+        std::sort(pairs.begin(), pairs.end());
+        for (uint64_t i = 0; i < m; ++i) {
+            out_offsets[i] = pairs[i].second;
+            if (out_jobs) out_jobs[i] = pairs[i].first;
+        }
+    }
+    return CMC_OK;
+}
+
+int Ctx::autotune(const cmc_job* in, uint32_t n, uint32_t sample_div) {
+    int rc = cuda(cudaSetDevice(device), "cudaSetDevice");
+    if (rc) return rc;
+    std::vector<Job> jobs;
+    std::vector<uint32_t> order;
+    uint64_t total = 0;
+    if ((rc = prepare_jobs(in, n, sample_div ? sample_div : 64, jobs, order, total))) return rc;
+    cudaStream_t st = user_stream ? user_stream : stream;
+    bool any_h_small = false;
+    for (const Job& j : jobs) any_h_small = any_h_small || j.half_bits <= 12;
+    std::vector<TunedPlan> cands;
+    for (int iso : {0, 1})
+        for (uint32_t wg : {1u, 2u, 4u, 6u})
+            for (int method : {-1, 0}) {
+                if (method == 0 && !any_h_small) continue;  // auto already picks direct
+                cands.push_back(TunedPlan{wg, iso, method});
+            }
+    if ((rc = grow(d_job_failed, job_failed_cap, n, "job counters"))) return rc;
+    double best_ms = 1e300;
+    TunedPlan best{};
+    std::string best_text;
+    for (const TunedPlan& t : cands) {
+        ScopedPlan scoped(*this, &t);
+        // rebuild methods under the candidate's method choice
+        std::vector<Job> js = jobs;
+        for (uint32_t i = 0; i < n; ++i) {
+            Job tmp;
+            if ((rc = make_job(in[order[i]].params, js[i].first, js[i].count, js[i].trial_base, tmp))) return rc;
+            js[i].method = tmp.method;
+        }
+        if ((rc = upload_jobs(js, st))) return rc;
+        rc = run(js, total, st, 0, nullptr, nullptr, 0, d_job_failed, nullptr);
+        if (rc == CMC_EINVAL) continue;  // plan does not fit: skip the candidate
+        if (rc) return rc;
+        float ms = 0;
+        if ((rc = cuda(cudaEventSynchronize(ev_stop), "tune sync"))) return rc;
+        if ((rc = cuda(cudaEventElapsedTime(&ms, ev_start, ev_stop), "tune time"))) return rc;
+        if ((rc = check_ctrl())) return rc;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+            best_text = plan_text;
+        }
+    }
+    if (best_ms == 1e300) return fail(CMC_EINVAL, "no candidate plan fits this mix");
+    tuned[mix_key(in, n)] = best;
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s | sample %.3f ms for %llu trials", best_text.c_str(), best_ms,
+             (unsigned long long)total);
+    tune_text = buf;
+    return CMC_OK;
 }
 
 }  // namespace cmc
@@ -458,6 +651,22 @@ int cmc_check(cmc_ctx* ctx) {
     int rc = c->cuda(cudaDeviceSynchronize(), "synchronize");
     if (rc) return rc;
     return c->check_ctrl();
+}
+
+int cmc_run_jobs(cmc_ctx* ctx, const cmc_job* jobs, uint32_t njobs, uint64_t* out_failed,
+                 uint32_t* out_offsets, uint32_t* out_jobs, uint64_t cap, uint64_t* out_total) {
+    if (!ctx) return CMC_EINVAL;
+    return reinterpret_cast<Ctx*>(ctx)->run_jobs(jobs, njobs, out_failed, out_offsets, out_jobs, cap,
+                                                  out_total);
+}
+
+int cmc_autotune(cmc_ctx* ctx, const cmc_job* jobs, uint32_t njobs, uint32_t sample_div,
+                 const char** out_choice) {
+    if (!ctx) return CMC_EINVAL;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    const int rc = c->autotune(jobs, njobs, sample_div);
+    if (out_choice) *out_choice = c->tune_text.c_str();
+    return rc;
 }
 
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {

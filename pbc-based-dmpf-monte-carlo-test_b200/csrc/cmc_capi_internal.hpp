@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -19,6 +20,13 @@ struct Plan {
     uint32_t slot_stride = 0, bins_bytes = 0, group_bytes = 0;
     uint32_t group_off = 0, slots_off = 0, smem_bytes = 0, threads = 0, ctas = 0;
     int variant = 0;  // 0: u16 map/bins, 1: u32 map/bins, 2: u32 + 64-bit PRP domain
+};
+
+// Planner options chosen by the autotuner for one mix of parameter sets.
+struct TunedPlan {
+    uint32_t wg = 0;
+    int isolate = -1;
+    int method = -1;
 };
 
 struct Ctx {
@@ -41,6 +49,10 @@ struct Ctx {
     GSlotHeader* d_ghdr = nullptr;
     size_t ghdr_cap = 0;
     uint32_t* d_key = nullptr;
+    unsigned long long* d_job_failed = nullptr;
+    size_t job_failed_cap = 0;
+    std::map<std::string, TunedPlan> tuned;  // autotuner results by job mix
+    std::string tune_text;
     std::string err, plan_text;
     uint32_t kernels = 0;
     Plan last_plan;
@@ -63,13 +75,19 @@ struct Ctx {
     int plan(const std::vector<Job>& jobs, Plan& pl);
     int upload_jobs(const std::vector<Job>& jobs, cudaStream_t st);
     int run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint32_t value_base,
-            uint32_t* d_out, uint32_t* d_count, unsigned long long* job_failed,
+            uint32_t* d_out, uint32_t* d_count, uint64_t out_cap, unsigned long long* job_failed,
             unsigned long long* job_done);
     int check_ctrl();
     int launch_host(const cmc_params& p, const uint32_t key[44], uint32_t first, uint32_t count,
                     uint32_t* out, uint32_t* nfailed);
     int launch_device(const cmc_params& p, const uint32_t* d_key, uint32_t first, uint32_t count,
                       uint32_t* d_offsets, uint32_t* d_nfailed, cudaStream_t st);
+    int prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::vector<Job>& out,
+                     std::vector<uint32_t>& order, uint64_t& total);
+    std::string mix_key(const cmc_job* in, uint32_t n) const;
+    int run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t* out_offsets,
+                 uint32_t* out_jobs, uint64_t cap, uint64_t* out_total);
+    int autotune(const cmc_job* in, uint32_t n, uint32_t sample_div);
 };
 
 }  // namespace cmc

@@ -805,11 +805,13 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
 }
 
 // Ordered failure list from the bitmap: one CTA, block-wide exclusive scan.
-// out[i] = value_base + (index of the i-th set bit); *count = number of bits.
+// out[i] = value_base + (index of the i-th set bit) for i < cap; *count = the
+// number of set bits.
 __global__ void __launch_bounds__(1024) cmc_compact_failures(const uint32_t* __restrict__ bits,
                                                              uint64_t nbits, uint32_t value_base,
                                                              uint32_t* __restrict__ out,
-                                                             uint32_t* __restrict__ count) {
+                                                             uint32_t* __restrict__ count,
+                                                             uint64_t cap) {
     __shared__ uint32_t warp_sums[32];
     const uint64_t words = (nbits + 31) / 32;
     const uint64_t per = (words + blockDim.x - 1) / blockDim.x;
@@ -841,7 +843,8 @@ __global__ void __launch_bounds__(1024) cmc_compact_failures(const uint32_t* __r
         while (b) {
             const int i = __ffs(b) - 1;
             b &= b - 1;
-            out[at++] = value_base + (uint32_t)(w * 32 + i);
+            if (at < cap) out[at] = value_base + (uint32_t)(w * 32 + i);
+            ++at;
         }
     }
 }

@@ -1,0 +1,51 @@
+"""Batched launches (cmc_run_jobs): every job's failures are identical alone
+(one cmc_launch per job) and in the mix, whatever the plan."""
+import random
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def random_mix(cmc, n, seed, small=False):
+    rng = random.Random(seed)
+    jobs = []
+    for _ in range(n):
+        pnum = rng.choice([16, 30, 64, 150, 300] if small else [16, 64, 300, 1024, 2500])
+        k = rng.choice([2, 3, 3, 4])
+        ell = rng.choice([16, 20, 24])
+        b = int(pnum * rng.choice([1.1, 1.25, 1.5]))
+        kick = rng.choice([50, 100, 500])
+        mode = rng.choice(["bgh25", "bgh25", "drrt18"])
+        im = rng.choice(["affine", "sequential"])
+        p = cmc.parameters(mode, pnum, ell, k, b, kick, im)
+        count = rng.choice([1, 7, 100, 513]) if pnum > 1000 else rng.choice([1, 33, 1000, 2048])
+        jobs.append((p, rng.randrange(1 << 32), rng.randrange(16), rng.randrange(1000), count))
+    return jobs
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_alone_equals_mix(ctx, cmc, seed):
+    jobs = random_mix(cmc, 12, seed)
+    failed, per_job = ctx.run_jobs(jobs)
+    for i, (p, s, b, first, count) in enumerate(jobs):
+        alone = ctx.launch(p, cmc.batch_key(s, b), first, count)
+        assert per_job[i] == alone, (i, ctx.last_plan)
+        assert failed[i] == len(alone)
+
+
+def test_autotuned_plan_keeps_results(ctx, cmc):
+    jobs = random_mix(cmc, 8, 5, small=True)
+    before, per_before = ctx.run_jobs(jobs)
+    choice = ctx.autotune(jobs, sample_div=8)
+    assert "engine=" in choice
+    after, per_after = ctx.run_jobs(jobs)
+    assert after == before and per_after == per_before
+
+
+def test_capacity_limits_offsets_not_counts(ctx, cmc):
+    jobs = [(cmc.parameters("bgh25", 64, 16, 3, 70, 20, "affine"), 3, 0, 0, 2000)]
+    failed, per_job = ctx.run_jobs(jobs, cap=5)
+    assert failed[0] > 5 and len(per_job[0]) == 5
+    full = ctx.launch(jobs[0][0], cmc.batch_key(3, 0), 0, 2000)
+    assert failed[0] == len(full)
