@@ -120,6 +120,34 @@ int cmc_run_jobs(cmc_ctx* ctx, const cmc_job* jobs, uint32_t njobs, uint64_t* ou
 int cmc_autotune(cmc_ctx* ctx, const cmc_job* jobs, uint32_t njobs, uint32_t sample_div,
                  const char** out_choice);
 
+/* Serving (no counterpart in the reference): estimation jobs of different
+ * sizes are submitted as they arrive and run together, continuously batched
+ * into the persistent engine.  Job state (parameters, RNG counter = next trial,
+ * budget, current batch key) and partial counts live on the device; each
+ * cmc_server_step admits queued jobs while the device-memory budget allows,
+ * grants trials (shortest remaining work first, a quarter of the step's work
+ * to the oldest job), runs one engine launch over all grants and appends
+ * completed batches to each job's v3 journal (when a directory was given; an
+ * existing journal there is resumed).  A budget runs as the first
+ * ceil(trials / 2^batch_bits) batches of an experiment of 2^ceil(log2 trials)
+ * trials, so it is rounded up to whole batches.  A job's failures are the
+ * same alone and in the mix. */
+typedef struct cmc_server cmc_server;
+int cmc_server_create(cmc_ctx* ctx, uint32_t max_jobs, uint64_t mem_budget_bytes,
+                      uint32_t batch_bits, uint64_t max_iteration_trials, cmc_server** out);
+int cmc_server_submit(cmc_server* server, const cmc_params* params, uint64_t seed,
+                      uint64_t trials, const char* journal_dir, uint32_t* out_id);
+/* One iteration; work_blocks is its AES-block budget.  Writes up to cap ids
+ * of jobs that finished in this step to out_finished. */
+int cmc_server_step(cmc_server* server, uint64_t work_blocks, uint32_t* out_finished,
+                    uint32_t cap, uint32_t* out_nfinished);
+/* out_state: 0 queued, 1 running, 2 done. */
+int cmc_server_status(cmc_server* server, uint32_t job_id, uint64_t* out_trials_done,
+                      uint64_t* out_failed, int* out_state);
+uint32_t cmc_server_pending(const cmc_server* server);
+const char* cmc_server_error(const cmc_server* server);
+int cmc_server_destroy(cmc_server* server);
+
 /* Tuning knobs of the launch planner; value 0 (or -1 for "method") restores
  * the automatic choice.  Names: "warps_per_group" (1..15), "groups" (1..14),
  * "global_slots" (0/1: keep walk slots in global memory), "method"

@@ -37,7 +37,8 @@ EXPORTS = (
     "cmc_last_error", "cmc_launch", "cmc_launch_device", "cmc_check",
     "cmc_last_kernel_count", "cmc_last_plan", "cmc_set_option",
     "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats", "cmc_launch_static",
-    "cmc_run_jobs", "cmc_autotune",
+    "cmc_run_jobs", "cmc_autotune", "cmc_server_create", "cmc_server_submit", "cmc_server_step",
+    "cmc_server_status", "cmc_server_pending", "cmc_server_error", "cmc_server_destroy",
 )
 
 
@@ -129,6 +130,20 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.cmc_run_jobs.restype = ctypes.c_int
     lib.cmc_autotune.argtypes = [vp, P(Job), u32, u32, P(ctypes.c_char_p)]
     lib.cmc_autotune.restype = ctypes.c_int
+    lib.cmc_server_create.argtypes = [vp, u32, u64, u32, u64, P(vp)]
+    lib.cmc_server_create.restype = ctypes.c_int
+    lib.cmc_server_submit.argtypes = [vp, P(Params), u64, u64, ctypes.c_char_p, P(u32)]
+    lib.cmc_server_submit.restype = ctypes.c_int
+    lib.cmc_server_step.argtypes = [vp, u64, P(u32), u32, P(u32)]
+    lib.cmc_server_step.restype = ctypes.c_int
+    lib.cmc_server_status.argtypes = [vp, u32, P(u64), P(u64), P(ctypes.c_int)]
+    lib.cmc_server_status.restype = ctypes.c_int
+    lib.cmc_server_pending.argtypes = [vp]
+    lib.cmc_server_pending.restype = u32
+    lib.cmc_server_error.argtypes = [vp]
+    lib.cmc_server_error.restype = ctypes.c_char_p
+    lib.cmc_server_destroy.argtypes = [vp]
+    lib.cmc_server_destroy.restype = ctypes.c_int
     lib.cmc_last_plan.argtypes = [vp]
     lib.cmc_last_plan.restype = ctypes.c_char_p
     if path is None:
@@ -277,6 +292,82 @@ class Context:
     @property
     def last_kernel_count(self) -> int:
         return self.lib.cmc_last_kernel_count(self.handle)
+
+
+class Server:
+    """Serving loop (cmc_server_*): jobs submitted as they arrive, continuously
+    batched into the persistent engine; state and counts stay on the device."""
+
+    def __init__(self, ctx: Context, max_jobs: int = 1024, mem_budget: int = 4 << 30,
+                 batch_bits: int = 20, max_iteration_trials: int = 1 << 22):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = ctypes.c_void_p()
+        rc = self.lib.cmc_server_create(ctx.handle, max_jobs, mem_budget, batch_bits,
+                                        max_iteration_trials, ctypes.byref(h))
+        if rc:
+            raise CmcError(rc, self.lib.cmc_last_error(ctx.handle).decode())
+        self.handle = h
+
+    def _raise(self, rc: int):
+        raise CmcError(rc, self.lib.cmc_server_error(self.handle).decode())
+
+    def submit(self, params: Params, seed: int, trials: int, journal_dir: str | None = None) -> int:
+        out = ctypes.c_uint32()
+        rc = self.lib.cmc_server_submit(self.handle, ctypes.byref(params), seed, trials,
+                                        journal_dir.encode() if journal_dir else None,
+                                        ctypes.byref(out))
+        if rc:
+            self._raise(rc)
+        return out.value
+
+    def step(self, work_blocks: int) -> list[int]:
+        cap = 4096
+        fin = (ctypes.c_uint32 * cap)()
+        n = ctypes.c_uint32()
+        rc = self.lib.cmc_server_step(self.handle, work_blocks, fin, cap, ctypes.byref(n))
+        if rc:
+            self._raise(rc)
+        return list(fin[: min(n.value, cap)])
+
+    def status(self, job: int) -> tuple[int, int, int]:
+        done, failed, state = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int()
+        rc = self.lib.cmc_server_status(self.handle, job, ctypes.byref(done), ctypes.byref(failed),
+                                        ctypes.byref(state))
+        if rc:
+            self._raise(rc)
+        return done.value, failed.value, state.value
+
+    def pending(self) -> int:
+        return self.lib.cmc_server_pending(self.handle)
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.cmc_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_journal(path: os.PathLike | str) -> dict[int, list[int]]:
+    """Committed records of a v3/v4 journal file: {batch: sorted failing offsets}."""
+    import struct
+    data = Path(path).read_bytes()
+    version = struct.unpack_from("<I", data, 4)[0]
+    at = 56 + (8 if version == 4 else 0)
+    out: dict[int, list[int]] = {}
+    while at + 16 <= len(data):
+        batch, tried, failed = struct.unpack_from("<QII", data, at)
+        end = at + 16 + 4 * failed + 8
+        if end > len(data):
+            break
+        out[batch] = list(struct.unpack_from(f"<{failed}I", data, at + 16))
+        at = end
+    return out
 
 
 STATIC_MAX_TRIALS = 1 << 20

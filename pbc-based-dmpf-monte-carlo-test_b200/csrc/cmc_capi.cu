@@ -22,7 +22,8 @@ __global__ void cmc_engine(const EngineArgs a);
 template <typename MapT, typename BinT, bool WIDE>
 __global__ void cmc_engine_split(const EngineArgs a);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
-                                     uint32_t* out, uint32_t* count, uint64_t cap);
+                                     uint32_t* out, uint32_t* count, uint64_t cap,
+                                     const unsigned long long* nbits_dev);
 __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out,
                              uint32_t r256);
 
@@ -275,7 +276,8 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     if ((rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
     kernels = 1;
     if (d_out) {
-        cmc_compact_failures<<<1, 1024, 0, st>>>(d_bits, total, value_base, d_out, d_count, out_cap_now);
+        cmc_compact_failures<<<1, 1024, 0, st>>>(d_bits, total, value_base, d_out, d_count, out_cap_now,
+                                                 nullptr);
         if ((rc = cuda(cudaGetLastError(), "compaction launch"))) return rc;
         kernels = 2;
     }

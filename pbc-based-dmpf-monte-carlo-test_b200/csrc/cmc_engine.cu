@@ -238,13 +238,14 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
     GroupHeader* gh = reinterpret_cast<GroupHeader*>(gbase);
     uint16_t* cache = reinterpret_cast<uint16_t*>(gbase + sizeof(GroupHeader));
     uint32_t cursor = 0;
+    const unsigned long long total = a.total_dev ? *a.total_dev : a.total;
 
     for (;;) {
         if (gt == 0) {
             const unsigned long long gi = atomicAdd(&a.ctrl->next, 1ULL);
             gh->gidx = gi;
             gh->abort = 0;
-            if (gi < a.total) {
+            if (gi < total) {
                 const uint32_t j = find_job(a.jobs, a.njobs, gi);
                 gh->job = j;
                 gh->offset = a.jobs[j].first + (uint32_t)(gi - a.jobs[j].trial_base);
@@ -252,7 +253,7 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         }
         group_sync(g, gthreads);
         const unsigned long long gi = gh->gidx;
-        if (gi >= a.total) break;
+        if (gi >= total) break;
         const Job& J = a.jobs[gh->job];
 
         // Per-trial PRP key and walk seed (cuckoo_bench.cu:226-238).
@@ -616,11 +617,12 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
                 atomicExch(&a.ctrl->error, kErrRange);
                 atomicExch(&a.ctrl->where, 3u);
             }
+            const uint32_t cidx = a.count_by_user ? a.jobs[job].user : job;
             if (w.failed) {
                 atomicOr(&a.fail_bits[gidx >> 5], 1u << (gidx & 31));
-                if (a.job_failed) atomicAdd(&a.job_failed[job], 1ULL);
+                if (a.job_failed) atomicAdd(&a.job_failed[cidx], 1ULL);
             }
-            if (a.job_done) atomicAdd(&a.job_done[job], 1ULL);
+            if (a.job_done) atomicAdd(&a.job_done[cidx], 1ULL);
             ++walks;
             busy = false;
             __threadfence_block();
@@ -697,11 +699,12 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
                 atomicExch(&a.ctrl->error, kErrRange);
                 atomicExch(&a.ctrl->where, 3u);
             }
+            const uint32_t cidx = a.count_by_user ? a.jobs[job].user : job;
             if (w.failed) {
                 atomicOr(&a.fail_bits[gidx >> 5], 1u << (gidx & 31));
-                if (a.job_failed) atomicAdd(&a.job_failed[job], 1ULL);
+                if (a.job_failed) atomicAdd(&a.job_failed[cidx], 1ULL);
             }
-            if (a.job_done) atomicAdd(&a.job_done[job], 1ULL);
+            if (a.job_done) atomicAdd(&a.job_done[cidx], 1ULL);
             ++walks;
             busy = false;
             __threadfence();
@@ -811,8 +814,10 @@ __global__ void __launch_bounds__(1024) cmc_compact_failures(const uint32_t* __r
                                                              uint64_t nbits, uint32_t value_base,
                                                              uint32_t* __restrict__ out,
                                                              uint32_t* __restrict__ count,
-                                                             uint64_t cap) {
+                                                             uint64_t cap,
+                                                             const unsigned long long* nbits_dev) {
     __shared__ uint32_t warp_sums[32];
+    if (nbits_dev) nbits = *nbits_dev;
     const uint64_t words = (nbits + 31) / 32;
     const uint64_t per = (words + blockDim.x - 1) / blockDim.x;
     const uint64_t w0 = per * threadIdx.x, w1 = min(words, w0 + per);

@@ -71,10 +71,40 @@ struct EngineArgs {
     // is walked by thread s of the walker CTAs; headers in global memory
     GSlotHeader* ghdr;
     uint32_t split, producer_ctas, total_groups;
+    // serving: the trial total is written by the scheduler kernel that runs
+    // just before (nullptr: use `total`), and per-job counters are indexed by
+    // Job::user (the server slot) rather than by table position
+    const unsigned long long* total_dev;
+    uint32_t count_by_user;
     uint32_t group_bytes;               // per-group smem (header + cache)
     uint32_t group_off;                 // smem offset of group 0
     uint32_t slots_off;                 // smem offset of slot 0 (smem slots)
     uint32_t spin_limit;                // bounded waits (polls of ~0.5 us)
+};
+
+// Serving: device-resident state of one admitted job.  `next` is the job's
+// RNG counter -- the index of its next trial in the experiment, whose batch
+// is next >> bt and offset next & (2^bt - 1); `job.batch_rk` caches the key of
+// batch `key_batch`.
+struct ServeState {
+    Job job;
+    unsigned long long seed;
+    unsigned long long next;
+    unsigned long long budget;
+    unsigned long long key_batch;
+    uint32_t bt, active;
+};
+
+// Serving: this iteration's share for one job.
+struct Grant {
+    uint32_t slot;
+    uint32_t trials;
+};
+
+// Serving: where each table entry of an iteration came from.
+struct GrantInfo {
+    unsigned long long batch, base;
+    uint32_t slot, first, count, pad;
 };
 
 }  // namespace cmc

@@ -37,7 +37,8 @@ namespace cmc {
 template <typename MapT, typename BinT, bool WIDE>
 __global__ void cmc_engine(const EngineArgs a);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
-                                     uint32_t* out, uint32_t* count, uint64_t cap);
+                                     uint32_t* out, uint32_t* count, uint64_t cap,
+                                     const unsigned long long* nbits_dev);
 void set_thread_error(const std::string& message);
 
 namespace {
@@ -200,7 +201,7 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
     e = cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, s);
     if (e != cudaSuccess) return fail(CMC_ECUDA, std::string("engine launch: ") + cudaGetErrorString(e));
     cmc_compact_failures<<<1, 1024, 0, s>>>(a.fail_bits, count, first, d_out_offsets, d_out_nfailed,
-                                            count);
+                                            count, nullptr);
     static_finish<<<1, 1, 0, s>>>(st->scratch, d_out_nfailed);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(CMC_ECUDA, std::string("compaction launch: ") + cudaGetErrorString(e));
