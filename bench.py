@@ -294,6 +294,104 @@ def run_sweep_workload(args):
     ctx.close()
 
 
+# ------------------------------------------------------------ serve workload --
+
+def serve_jobs(n_jobs: int, rate: float, log2_budget: tuple[float, float], draw_seed: int = 5):
+    """The served stream: Poisson arrivals at `rate` jobs/s; t = round(2^U[4,14]),
+    B = ceil(r t) with r in {1.2, 1.3, 1.4, 1.5}, k in {2, 3}, max kicks 500,
+    N = 2^24, budget = round(2^U[log2_budget]) trials; job i has seed
+    draw_seed*100000 + i.  The budget range is a parameter because the full
+    range (2^16..2^24) is about an hour of GPU work."""
+    import numpy as np
+    rng = np.random.default_rng(draw_seed)
+    t_arr = 0.0
+    jobs = []
+    for i in range(n_jobs):
+        t_arr += float(rng.exponential(1.0 / rate))
+        t = int(round(2 ** rng.uniform(4, 14)))
+        r = float(rng.choice([1.2, 1.3, 1.4, 1.5]))
+        k = int(rng.choice([2, 3]))
+        budget = int(round(2 ** rng.uniform(*log2_budget)))
+        jobs.append(dict(arrival=t_arr, mode="bgh25", pnum=max(t, 3), ell_i=24, k=k,
+                         buckets=math.ceil(r * t), kick=500, input_mode="affine",
+                         seed=draw_seed * 100000 + i, trials=budget))
+    return jobs
+
+
+def rounded_budget(trials: int, bt_max: int = 20):
+    et = max(1, (trials - 1).bit_length())
+    bt = min(bt_max, et)
+    per = 1 << bt
+    return -(-trials // per) * per, bt
+
+
+def run_serve_workload(args):
+    """Served (continuous batching) vs plain (one launch per job, in arrival
+    order) on the same job stream; job latency = completion - arrival."""
+    cmc = load_pkg()
+    ctx = cmc.Context(0)
+    lo, hi = (float(x) for x in args.serve_log2_budget.split(","))
+    jobs = serve_jobs(args.serve_jobs, args.serve_rate, (lo, hi))
+    params = [cmc.parameters(j["mode"], j["pnum"], j["ell_i"], j["k"], j["buckets"], j["kick"],
+                             j["input_mode"]) for j in jobs]
+    total_trials = sum(rounded_budget(j["trials"])[0] for j in jobs)
+
+    # served
+    srv = cmc.Server(ctx, max_jobs=4096, mem_budget=8 << 30, batch_bits=20,
+                     max_iteration_trials=1 << 23)
+    t0 = time.perf_counter()
+    submitted, done_at, ids = 0, {}, {}
+    while len(done_at) < len(jobs):
+        now = time.perf_counter() - t0
+        while submitted < len(jobs) and jobs[submitted]["arrival"] <= now:
+            j = jobs[submitted]
+            ids[srv.submit(params[submitted], j["seed"], j["trials"])] = submitted
+            submitted += 1
+        if srv.pending():
+            for jid in srv.step(args.serve_step_blocks):
+                done_at[ids[jid]] = time.perf_counter() - t0
+        elif submitted < len(jobs):
+            time.sleep(max(0.0, jobs[submitted]["arrival"] - (time.perf_counter() - t0)))
+    served_span = time.perf_counter() - t0
+    served_failed = [srv.status(jid)[1] for jid in sorted(ids, key=lambda x: ids[x])]
+    srv.close()
+    lat_served = sorted(done_at[i] - jobs[i]["arrival"] for i in range(len(jobs)))
+
+    # plain: each job alone, one launch covering its batches, arrival order
+    t0 = time.perf_counter()
+    lat_plain, plain_failed = [], []
+    for i, j in enumerate(jobs):
+        now = time.perf_counter() - t0
+        if j["arrival"] > now:
+            time.sleep(j["arrival"] - now)
+        budget, bt = rounded_budget(j["trials"])
+        per = 1 << bt
+        entries = [(params[i], j["seed"], b, 0, per) for b in range(budget // per)]
+        counts, _ = ctx.run_jobs(entries, cap=0)
+        plain_failed.append(sum(counts))
+        lat_plain.append(time.perf_counter() - t0 - j["arrival"])
+    plain_span = time.perf_counter() - t0
+    lat_plain.sort()
+
+    def pct(v, q):
+        return v[min(len(v) - 1, int(q * len(v)))]
+
+    line = {
+        "metric": "served stream: job latency p50/p99 (s) and trials/s, served vs plain",
+        "workload": f"{len(jobs)} jobs, Poisson {args.serve_rate}/s, budgets 2^U[{lo},{hi}] "
+                    f"(rounded up to whole batches), t = 2^U[4,14], N = 2^24, seed 5",
+        "served": {"p50_s": pct(lat_served, 0.5), "p99_s": pct(lat_served, 0.99),
+                   "trials_per_s": total_trials / served_span, "makespan_s": served_span},
+        "plain": {"p50_s": pct(lat_plain, 0.5), "p99_s": pct(lat_plain, 0.99),
+                  "trials_per_s": total_trials / plain_span, "makespan_s": plain_span},
+        "identical_failure_counts": served_failed == plain_failed,
+        "total_trials": total_trials, "step_blocks": args.serve_step_blocks,
+        "timing": "host wall clock from each job's arrival to its completion",
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 # ------------------------------------------------------------------ our arm --
 
 def main():
@@ -305,7 +403,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--trials", type=int, default=1 << 20,
                     help="trials per step (default one batch, 2^20); smaller for profiling")
-    ap.add_argument("--workload", choices=["config2", "sweep"], default="config2")
+    ap.add_argument("--workload", choices=["config2", "sweep", "serve"], default="config2")
+    ap.add_argument("--serve-jobs", type=int, default=400)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-log2-budget", default="10,16")
+    ap.add_argument("--serve-step-blocks", type=int, default=400_000_000)
     ap.add_argument("--sweep-trials", type=int, default=1 << 16,
                     help="trials per parameter set for --workload sweep")
     args = ap.parse_args()
@@ -320,6 +422,10 @@ def main():
     if args.workload == "sweep":
         if rank == 0:
             run_sweep_workload(args)
+        return
+    if args.workload == "serve":
+        if rank == 0:
+            run_serve_workload(args)
         return
 
     import torch
