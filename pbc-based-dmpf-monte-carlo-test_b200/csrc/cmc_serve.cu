@@ -124,6 +124,8 @@ struct HostJob {
     double cost = 1;  // estimated AES blocks per trial
     uint64_t failed = 0;
     uint64_t admitted_at = 0;  // iteration number
+    int global_slots = 0;      // 1: its table needs walk slots in global memory
+    double latency_blocks = 0; // one trial's latency, in AES blocks of GPU throughput
     // failing offsets per uncommitted batch, and the journal
     std::vector<std::pair<uint64_t, std::vector<uint32_t>>> pending;
     std::unique_ptr<Journal> journal;
@@ -256,6 +258,18 @@ struct Server {
         const double c = std::ldexp(1.0, 2 * int(p.half_bits)) / double(p.domain);
         j.cost = 2.0 + std::min(8.0 * std::ldexp(1.0, int(p.half_bits)), 8.0 * p.k * p.pnum * c) +
                  0.3 * p.pnum;
+        {
+            // size class: do this table's walk slots fit in shared memory?
+            std::vector<Job> one(1);
+            one[0] = probe;
+            Plan pl;
+            if ((rc = ctx->plan(one, pl))) return fail(rc, ctx->err);
+            j.global_slots = pl.slots_smem ? 0 : 1;
+            // a trial's walk is ~2.4 t probes of ~300 (shared) or ~1300 (global)
+            // cycles; expressed in blocks of GPU throughput (~4e10 blocks/s at 2 GHz)
+            const double walk_cycles = 2.4 * p.pnum * (j.global_slots ? 1300.0 : 300.0);
+            j.latency_blocks = walk_cycles / 2.0e9 * 4.0e10;
+        }
         if (journal_dir && *journal_dir) {
             Options& o = j.jopt;
             o.mode = p.mode == CMC_MODE_BGH25 ? "bgh25" : "drrt18";
@@ -345,19 +359,34 @@ struct Server {
         int rc = cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
         if (rc) return rc;
         if ((rc = admit())) return rc;
-        std::vector<uint32_t> ids = active_ids();
-        if (ids.empty()) return CMC_OK;
-        // grants: a quarter of the work to the oldest job, the rest shortest
-        // remaining work first
+        std::vector<uint32_t> all = active_ids();
+        if (all.empty()) return CMC_OK;
+        // One size class per step, so the plan keeps shared-memory walk slots
+        // whenever the granted tables allow: the class of the job with the
+        // least remaining work, and every 4th step the class of the oldest job.
+        uint32_t oldest = all[0], smallest = all[0];
+        auto remaining = [&](uint32_t id) { return double(jobs[id].budget - jobs[id].next) * jobs[id].cost; };
+        for (uint32_t id : all) {
+            if (jobs[id].admitted_at < jobs[oldest].admitted_at) oldest = id;
+            if (remaining(id) < remaining(smallest)) smallest = id;
+        }
+        const int cls = (iteration % 4 == 3) ? jobs[oldest].global_slots : jobs[smallest].global_slots;
+        std::vector<uint32_t> ids;
+        for (uint32_t id : all)
+            if (jobs[id].global_slots == cls) ids.push_back(id);
+        // grants: a quarter of the work to the oldest job of the class, the
+        // rest shortest remaining work first; the step is at least 2.5x the
+        // latency of its slowest trial so that trial's tail is covered
         std::vector<Grant> grants;
         std::vector<uint32_t> order = ids;
-        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-            return double(jobs[a].budget - jobs[a].next) * jobs[a].cost <
-                   double(jobs[b].budget - jobs[b].next) * jobs[b].cost;
-        });
-        uint32_t oldest = ids[0];
-        for (uint32_t id : ids)
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return remaining(a) < remaining(b); });
+        oldest = ids[0];
+        double floor_blocks = 0;
+        for (uint32_t id : ids) {
             if (jobs[id].admitted_at < jobs[oldest].admitted_at) oldest = id;
+            floor_blocks = std::max(floor_blocks, 2.5 * jobs[id].latency_blocks);
+        }
+        work_blocks = std::max<uint64_t>(work_blocks, uint64_t(floor_blocks));
         // shares per job (trials), then one grant per job
         std::vector<uint64_t> share(ids.size(), 0);
         std::vector<uint32_t> pos(jobs.size(), 0);
