@@ -125,8 +125,9 @@ int cmc_autotune(cmc_ctx* ctx, const cmc_job* jobs, uint32_t njobs, uint32_t sam
  * into the persistent engine.  Job state (parameters, RNG counter = next trial,
  * budget, current batch key) and partial counts live on the device; each
  * cmc_server_step admits queued jobs while the device-memory budget allows,
- * grants trials (shortest remaining work first, a quarter of the step's work
- * to the oldest job), runs one engine launch over all grants and appends
+ * grants trials to one size class of jobs (half of the step's work in arrival
+ * order, half shortest remaining work first), runs one engine launch over all
+ * grants and appends
  * completed batches to each job's v3 journal (when a directory was given; an
  * existing journal there is resumed).  A budget runs as the first
  * ceil(trials / 2^batch_bits) batches of an experiment of 2^ceil(log2 trials)

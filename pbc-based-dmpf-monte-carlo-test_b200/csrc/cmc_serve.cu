@@ -7,8 +7,9 @@
 // (the engine's per-job counters, indexed by server slot).  One iteration
 // (`cmc_server_step`):
 //   1. admits queued jobs while their slot memory fits the device-memory budget;
-//   2. grants each active job a number of trials: shortest remaining work first,
-//      with a share reserved for the oldest job so no job starves;
+//   2. picks one size class (jobs whose walk slots fit in shared memory, or
+//      not) and grants its jobs trials: half of the step's work in arrival
+//      order, so no job starves, half shortest remaining work first;
 //   3. the scheduler kernel turns the grants into the engine's job table on the
 //      device -- clamping at batch ends, deriving a batch key with device AES
 //      when a job enters a new batch, advancing the RNG counters, prefix-summing
@@ -362,30 +363,27 @@ struct Server {
         std::vector<uint32_t> all = active_ids();
         if (all.empty()) return CMC_OK;
         // One size class per step, so the plan keeps shared-memory walk slots
-        // whenever the granted tables allow: the class of the job with the
-        // least remaining work, and every 4th step the class of the oldest job.
+        // whenever the granted tables allow: alternately the class of the
+        // oldest job and the class of the job with the least remaining work.
         uint32_t oldest = all[0], smallest = all[0];
         auto remaining = [&](uint32_t id) { return double(jobs[id].budget - jobs[id].next) * jobs[id].cost; };
         for (uint32_t id : all) {
             if (jobs[id].admitted_at < jobs[oldest].admitted_at) oldest = id;
             if (remaining(id) < remaining(smallest)) smallest = id;
         }
-        const int cls = (iteration % 4 == 3) ? jobs[oldest].global_slots : jobs[smallest].global_slots;
+        const int cls = (iteration % 2 == 1) ? jobs[oldest].global_slots : jobs[smallest].global_slots;
         std::vector<uint32_t> ids;
         for (uint32_t id : all)
             if (jobs[id].global_slots == cls) ids.push_back(id);
-        // grants: a quarter of the work to the oldest job of the class, the
-        // rest shortest remaining work first; the step is at least 2.5x the
-        // latency of its slowest trial so that trial's tail is covered
+        // grants: half of the work in arrival order (bounds the tail), the rest
+        // shortest remaining work first (small jobs finish at once); the step
+        // is at least 2.5x the latency of its slowest trial so that trial's
+        // tail is covered
         std::vector<Grant> grants;
         std::vector<uint32_t> order = ids;
         std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return remaining(a) < remaining(b); });
-        oldest = ids[0];
         double floor_blocks = 0;
-        for (uint32_t id : ids) {
-            if (jobs[id].admitted_at < jobs[oldest].admitted_at) oldest = id;
-            floor_blocks = std::max(floor_blocks, 2.5 * jobs[id].latency_blocks);
-        }
+        for (uint32_t id : ids) floor_blocks = std::max(floor_blocks, 2.5 * jobs[id].latency_blocks);
         work_blocks = std::max<uint64_t>(work_blocks, uint64_t(floor_blocks));
         // shares per job (trials), then one grant per job
         std::vector<uint64_t> share(ids.size(), 0);
@@ -409,7 +407,14 @@ struct Server {
             trials_left -= n;
             left -= double(n) * j.cost;
         };
-        give(oldest, double(work_blocks) / 4.0);
+        std::vector<uint32_t> fifo = ids;
+        std::sort(fifo.begin(), fifo.end(), [&](uint32_t a, uint32_t b) {
+            return jobs[a].admitted_at != jobs[b].admitted_at ? jobs[a].admitted_at < jobs[b].admitted_at : a < b;
+        });
+        for (uint32_t id : fifo) {
+            if (left <= double(work_blocks) / 2.0 || trials_left == 0) break;
+            give(id, left - double(work_blocks) / 2.0);
+        }
         for (uint32_t id : order) {
             if (left <= 0 || trials_left == 0) break;
             give(id, left);
