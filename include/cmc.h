@@ -145,6 +145,10 @@ int cmc_server_step(cmc_server* server, uint64_t work_blocks, uint32_t* out_fini
 /* out_state: 0 queued, 1 running, 2 done. */
 int cmc_server_status(cmc_server* server, uint32_t job_id, uint64_t* out_trials_done,
                       uint64_t* out_failed, int* out_state);
+/* Share (0..1, default 0.5) of each step's work granted in arrival order;
+ * the rest goes shortest remaining work first.  1 is FIFO with backfill
+ * (tail latency of plain per-job launches), lower shares favour short jobs. */
+int cmc_server_policy(cmc_server* server, double fifo_share);
 uint32_t cmc_server_pending(const cmc_server* server);
 const char* cmc_server_error(const cmc_server* server);
 int cmc_server_destroy(cmc_server* server);

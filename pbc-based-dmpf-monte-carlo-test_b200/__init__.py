@@ -39,6 +39,7 @@ EXPORTS = (
     "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats", "cmc_launch_static",
     "cmc_run_jobs", "cmc_autotune", "cmc_server_create", "cmc_server_submit", "cmc_server_step",
     "cmc_server_status", "cmc_server_pending", "cmc_server_error", "cmc_server_destroy",
+    "cmc_server_policy",
 )
 
 
@@ -138,6 +139,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.cmc_server_step.restype = ctypes.c_int
     lib.cmc_server_status.argtypes = [vp, u32, P(u64), P(u64), P(ctypes.c_int)]
     lib.cmc_server_status.restype = ctypes.c_int
+    lib.cmc_server_policy.argtypes = [vp, ctypes.c_double]
+    lib.cmc_server_policy.restype = ctypes.c_int
     lib.cmc_server_pending.argtypes = [vp]
     lib.cmc_server_pending.restype = u32
     lib.cmc_server_error.argtypes = [vp]
@@ -340,6 +343,11 @@ class Server:
 
     def pending(self) -> int:
         return self.lib.cmc_server_pending(self.handle)
+
+    def policy(self, fifo_share: float) -> None:
+        rc = self.lib.cmc_server_policy(self.handle, fifo_share)
+        if rc:
+            self._raise(rc)
 
     def close(self) -> None:
         if self.handle:

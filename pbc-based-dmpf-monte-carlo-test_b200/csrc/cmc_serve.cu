@@ -155,6 +155,7 @@ struct Server {
     std::deque<uint32_t> queue;
     std::vector<uint32_t> free_slots;
     uint64_t fixed_bytes = 0;
+    double fifo_share = 0.5;  // part of each step's work granted in arrival order
     std::string err;
 
     int fail(int code, const std::string& m) {
@@ -411,9 +412,10 @@ struct Server {
         std::sort(fifo.begin(), fifo.end(), [&](uint32_t a, uint32_t b) {
             return jobs[a].admitted_at != jobs[b].admitted_at ? jobs[a].admitted_at < jobs[b].admitted_at : a < b;
         });
+        const double keep = double(work_blocks) * (1.0 - fifo_share);
         for (uint32_t id : fifo) {
-            if (left <= double(work_blocks) / 2.0 || trials_left == 0) break;
-            give(id, left - double(work_blocks) / 2.0);
+            if (left <= keep || trials_left == 0) break;
+            give(id, left - keep);
         }
         for (uint32_t id : order) {
             if (left <= 0 || trials_left == 0) break;
@@ -600,6 +602,12 @@ int cmc_server_status(cmc_server* server, uint32_t job_id, uint64_t* out_trials_
                       uint64_t* out_failed, int* out_state) {
     if (!server) return CMC_EINVAL;
     return reinterpret_cast<Server*>(server)->status(job_id, out_trials_done, out_failed, out_state);
+}
+
+int cmc_server_policy(cmc_server* server, double fifo_share) {
+    if (!server || !(fifo_share >= 0.0 && fifo_share <= 1.0)) return CMC_EINVAL;
+    reinterpret_cast<Server*>(server)->fifo_share = fifo_share;
+    return CMC_OK;
 }
 
 uint32_t cmc_server_pending(const cmc_server* server) {
