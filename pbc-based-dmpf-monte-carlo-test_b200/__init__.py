@@ -39,7 +39,7 @@ EXPORTS = (
     "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats", "cmc_launch_static",
     "cmc_run_jobs", "cmc_autotune", "cmc_server_create", "cmc_server_submit", "cmc_server_step",
     "cmc_server_status", "cmc_server_pending", "cmc_server_error", "cmc_server_destroy",
-    "cmc_server_policy",
+    "cmc_server_policy", "cmc_server_get_stats",
 )
 
 
@@ -143,6 +143,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.cmc_server_policy.restype = ctypes.c_int
     lib.cmc_server_pending.argtypes = [vp]
     lib.cmc_server_pending.restype = u32
+    lib.cmc_server_get_stats.argtypes = [vp, vp]
+    lib.cmc_server_get_stats.restype = ctypes.c_int
     lib.cmc_server_error.argtypes = [vp]
     lib.cmc_server_error.restype = ctypes.c_char_p
     lib.cmc_server_destroy.argtypes = [vp]
@@ -297,6 +299,12 @@ class Context:
         return self.lib.cmc_last_kernel_count(self.handle)
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_uint64), ("trials", ctypes.c_uint64),
+                ("engine_ms", ctypes.c_double), ("busy_ms", ctypes.c_double),
+                ("span_ms", ctypes.c_double)]
+
+
 class Server:
     """Serving loop (cmc_server_*): jobs submitted as they arrive, continuously
     batched into the persistent engine; state and counts stay on the device."""
@@ -344,15 +352,26 @@ class Server:
     def pending(self) -> int:
         return self.lib.cmc_server_pending(self.handle)
 
+    def stats(self) -> dict:
+        """Device-time accounting of the iterations read back so far."""
+        out = ServerStats()
+        rc = self.lib.cmc_server_get_stats(self.handle, ctypes.byref(out))
+        if rc:
+            self._raise(rc)
+        return {name: getattr(out, name) for name, _ in ServerStats._fields_}
+
     def policy(self, fifo_share: float) -> None:
         rc = self.lib.cmc_server_policy(self.handle, fifo_share)
         if rc:
             self._raise(rc)
 
     def close(self) -> None:
+        """Commits the iterations still in flight, then frees the server."""
         if self.handle:
-            self.lib.cmc_server_destroy(self.handle)
+            rc = self.lib.cmc_server_destroy(self.handle)
             self.handle = None
+            if rc:
+                raise CmcError(rc, self.lib.cmc_last_error(self.ctx.handle).decode())
 
     def __del__(self):
         try:

@@ -31,7 +31,6 @@ namespace {
 
 thread_local std::string g_thread_error;
 
-constexpr uint32_t kCtaSharedBytes = 2048;
 constexpr uint32_t kGroupHeaderBytes = 512;
 
 uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
@@ -70,6 +69,25 @@ int Ctx::grow(T*& ptr, size_t& cap, size_t need, const char* what) {
     return CMC_OK;
 }
 
+// Map method of a parameter set.  Direct passes cost 8 AES blocks per Feistel
+// evaluation, k*t*c evaluations per trial (c = 2^2h / D for cycle-walking).  A
+// round cache costs 8 * 2^h blocks per trial and then 8 lookups per
+// evaluation: from shared memory (h <= 12, a lookup ~1/64 block) or from an
+// L2-resident global buffer (h <= 16; ~0.3 block: the 8 lookups of an
+// evaluation are dependent L2 round trips, two chains in flight per lane).
+uint32_t choose_method(uint32_t h, uint64_t domain, double candidates, int force, bool may_allocate) {
+    const double c = std::ldexp(1.0, 2 * int(h)) / double(domain);
+    const double direct = candidates * 8.0 * c;
+    const double build = 8.0 * std::ldexp(1.0, int(h));
+    const bool gcache_ok = may_allocate && domain <= 0xffffffffULL && h <= 16;
+    if (force == 0) return kMethodDirect;
+    if (force == 1) return h <= 12 ? kMethodCache : gcache_ok ? kMethodGCache : kMethodDirect;
+    if (force == 2) return gcache_ok ? kMethodGCache : kMethodDirect;
+    if (h <= 12 && build + direct / 64.0 < direct) return kMethodCache;
+    if (gcache_ok && build + direct * 0.3 < direct) return kMethodGCache;
+    return kMethodDirect;
+}
+
 // Fill a device job descriptor from derived parameters.
 int Ctx::make_job(const cmc_params& p, uint32_t first, uint32_t count, uint64_t base, Job& j) {
     std::memset(&j, 0, sizeof j);
@@ -100,19 +118,14 @@ int Ctx::make_job(const cmc_params& p, uint32_t first, uint32_t count, uint64_t 
     j.first = first;
     j.count = count;
     j.trial_base = base;
-    // Round cache when it costs fewer AES blocks than direct passes and fits
-    // a group's shared memory (8 * 2^h u16 entries, h <= 12).
-    const double c = std::ldexp(1.0, 2 * int(p.half_bits)) / double(p.domain);
-    const double direct = double(p.pnum) * p.k * 8.0 * c;
-    const double cache = 8.0 * std::ldexp(1.0, int(p.half_bits)) + direct / 64.0;
-    j.method = (p.half_bits <= 12 && cache < direct && force_method != 0) ? kMethodCache : kMethodDirect;
-    if (force_method == 1 && p.half_bits <= 12) j.method = kMethodCache;
+    j.method = choose_method(p.half_bits, p.domain, double(p.pnum) * p.k, force_method, may_allocate);
     return CMC_OK;
 }
 
 // Choose groups, warps per group and slot placement for a set of jobs.
 int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     uint32_t max_b = 0, max_cand = 0, max_cache_h = 0, any_cache = 0, wide = 0, wide_domain = 0;
+    uint32_t max_gcache_h = 0, any_gcache = 0;
     double work = 0, cand_work = 0;
     for (const Job& j : jobs) {
         max_b = std::max(max_b, j.buckets);
@@ -120,6 +133,10 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
         if (j.method == kMethodCache) {
             any_cache = 1;
             max_cache_h = std::max(max_cache_h, j.half_bits);
+        }
+        if (j.method == kMethodGCache) {
+            any_gcache = 1;
+            max_gcache_h = std::max(max_gcache_h, j.half_bits);
         }
         if (j.domain > 0xffffffffULL) wide_domain = 1;
         // 16-bit entries: 14-bit ordinal + 2-bit choice, never equal to 0xffff
@@ -137,7 +154,7 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     const uint32_t cache_bytes = any_cache ? (16u << max_cache_h) : 0;
     pl.group_bytes = kGroupHeaderBytes + cache_bytes;
     const double avg_cand = work > 0 ? cand_work / work : 0;
-    pl.wg = (any_cache || avg_cand >= 768.0) ? 4 : 1;
+    pl.wg = (any_cache || any_gcache || avg_cand >= 768.0) ? 4 : 1;
     if (force_wg) pl.wg = force_wg;
     pl.walker_ctas = force_walker_ctas > 0 ? uint32_t(force_walker_ctas) : 0;
     if (pl.walker_ctas >= uint32_t(sms)) return fail(CMC_EINVAL, "walker_ctas must be below the SM count");
@@ -151,23 +168,40 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.nw = pl.walker_ctas ? 0 : (force_walkers ? force_walkers : 1);
     // measured best with isolated walkers: 2 groups of 6 producer warps on
     // sub-partitions 0..2 (2 x 7, adding two beside the walker, is within 3%)
-    if (pl.isolate && !force_wg) pl.wg = any_cache ? 6 : 4;
+    if (pl.isolate && !force_wg) pl.wg = (any_cache || any_gcache) ? 6 : 4;
     if (pl.isolate && pl.nw > 4) pl.nw = 4;
-    const uint32_t max_producer_warps = 16 - pl.nw;
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
-    uint32_t ng = std::min<uint32_t>(kMaxGroups, max_producer_warps / pl.wg);
-    if (force_ng) ng = std::min(ng, force_ng);
-    while (ng > 1 && ng * pl.group_bytes > budget) --ng;
+    auto groups_for = [&](uint32_t nw) {
+        uint32_t ng = std::min<uint32_t>(kMaxGroups, (16 - nw) / pl.wg);
+        if (force_ng) ng = std::min(ng, force_ng);
+        while (ng > 1 && ng * pl.group_bytes > budget) --ng;
+        return ng;
+    };
+    const uint32_t ng = groups_for(pl.nw);
     if (ng * pl.group_bytes > budget)
         return fail(CMC_EINVAL, "round cache of %u bytes does not fit shared memory", cache_bytes);
-    // Slots: 2..8 per group in shared memory when that fits without giving up
-    // more than half of the groups; otherwise up to 32 in global memory.
-    // The split engine keeps one global slot per walker-CTA thread.
+    // Slots.  A CTA walks about slots / (probes per trial x probe latency)
+    // trials per cycle: ~2.4 t probes per trial, ~300 cycles per probe in
+    // shared memory, ~3000 in global memory (two dependent DRAM round trips
+    // once the slots outgrow L2).  Its producers build AES blocks at a
+    // measured ~0.157 per cycle (direct passes, shared-memory cache) or ~0.2
+    // (global round cache), over the job's blocks per trial.  Shared-memory
+    // slots (2..8 per group, giving up at most half of the groups) are kept
+    // when their walks outpace the producers by 1.4x -- a small pool with
+    // uneven walk lengths queues below that -- or beat global slots; global
+    // slots take 32 per walker warp, with 4 walker warps on sub-partition 3
+    // when walkers are isolated.  The split engine keeps one global slot per
+    // walker-CTA thread.
+    double avg_cost = 0;
+    for (const Job& j : jobs) avg_cost += double(j.count) * job_cost(j);
+    avg_cost = work > 0 ? avg_cost / work : 1;
+    const double probes = std::max(1.0, 2.4 * avg_probe_work);
+    const double produce = (any_gcache ? 0.2 : 0.157) / std::max(1.0, avg_cost);
     pl.slots_smem = false;
     for (uint32_t g = ng; !pl.walker_ctas && !force_global_slots &&
                           g >= std::max<uint32_t>(1, (ng + 1) / 2); --g) {
         const uint32_t left = budget - g * pl.group_bytes;
-        const uint32_t s = std::min<uint32_t>({left / pl.slot_stride / g, kMaxSlots / g,
+        const uint32_t s = std::min<uint32_t>({left / pl.slot_stride / g, 32 * pl.nw / g,
                                                max_slots_per_group});
         if (s >= 2) {
             pl.ng = g;
@@ -179,9 +213,20 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     if (pl.walker_ctas) {
         pl.ng = ng;
         pl.ns = pl.walker_ctas * pl.ng * pl.wg * 32;
-    } else if (!pl.slots_smem) {
-        pl.ng = ng;
-        pl.ns = std::max<uint32_t>(1, kMaxSlots / ng) * ng;
+    } else {
+        const uint32_t nw_g = (pl.isolate && !force_walkers) ? 4 : pl.nw;
+        const uint32_t ng_g = groups_for(nw_g);
+        const uint32_t ns_g = std::max<uint32_t>(1, std::min(kMaxSlots, 32 * nw_g) / ng_g) * ng_g;
+        const double walk_smem = pl.slots_smem ? pl.ns / (probes * 300.0) : 0.0;
+        const double walk_global = ns_g / (probes * 3000.0);
+        const bool keep_smem = pl.slots_smem && (!may_allocate || walk_smem >= 1.4 * produce ||
+                                                 walk_smem >= walk_global);
+        if (!keep_smem) {
+            pl.slots_smem = false;
+            pl.nw = nw_g;
+            pl.ng = ng_g;
+            pl.ns = ns_g;
+        }
     }
     pl.group_off = kEngineTableBytes + kCtaSharedBytes;
     pl.slots_off = pl.group_off + pl.ng * pl.group_bytes;
@@ -192,6 +237,11 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
         pl.threads = (pl.ng * pl.wg + pl.nw) * 32;
     }
     pl.ctas = sms;
+    pl.gslot_bytes = pl.walker_ctas  ? uint64_t(pl.ns) * pl.slot_stride
+                     : pl.slots_smem ? 0
+                                     : uint64_t(pl.ctas) * pl.ns * pl.slot_stride;
+    pl.gcache_stride = any_gcache ? (8u << max_gcache_h) : 0;
+    pl.gcache_bytes = uint64_t(pl.ctas) * pl.ng * pl.gcache_stride * 2;
     char buf[256];
     snprintf(buf, sizeof buf,
              "engine=%s variant=%s groups=%u warps_per_group=%u walkers=%u%s slots=%u slots_in=%s "
@@ -199,7 +249,7 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
              pl.walker_ctas ? "split" : "group", pl.variant == 0 ? "narrow" : pl.variant == 1 ? "wide" : "wide-domain", pl.ng, pl.wg,
              pl.walker_ctas ? pl.walker_ctas : pl.nw, pl.isolate ? "(isolated)" : "", pl.ns,
              pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
-             any_cache ? "on" : "off");
+             any_cache && any_gcache ? "smem+global" : any_cache ? "smem" : any_gcache ? "global" : "off");
     plan_text = buf;
     return CMC_OK;
 }
@@ -214,14 +264,14 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     if (rc) return rc;
     const size_t words = (total + 31) / 32;
     if ((rc = grow(d_bits, bits_cap, words, "failure bitmap"))) return rc;
+    // one global pool: walk slots, then the groups' round caches
+    const size_t cache_off = size_t((pl.gslot_bytes + 255) / 256 * 256);
+    if (pl.gslot_bytes || pl.gcache_bytes)
+        if ((rc = grow(d_slots, slots_cap, cache_off + pl.gcache_bytes, "slot and cache pool"))) return rc;
     if (pl.walker_ctas) {
-        if ((rc = grow(d_slots, slots_cap, size_t(pl.ns) * pl.slot_stride, "slot pool"))) return rc;
         if ((rc = grow(d_ghdr, ghdr_cap, pl.ns, "slot headers"))) return rc;
         if ((rc = cuda(cudaMemsetAsync(d_ghdr, 0, size_t(pl.ns) * sizeof(GSlotHeader), st), "memset slots")))
             return rc;
-    } else if (!pl.slots_smem) {
-        const size_t need = size_t(pl.ctas) * pl.ns * pl.slot_stride;
-        if ((rc = grow(d_slots, slots_cap, need, "slot pool"))) return rc;
     }
     if ((rc = cuda(cudaMemsetAsync(d_ctrl, 0, sizeof(Ctrl), st), "memset ctrl"))) return rc;
     if ((rc = cuda(cudaMemsetAsync(d_bits, 0, words * 4, st), "memset bitmap"))) return rc;
@@ -234,6 +284,8 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     a.job_failed = job_failed;
     a.job_done = job_done;
     a.gslots = pl.slots_smem ? nullptr : d_slots;
+    a.gcache = pl.gcache_bytes ? reinterpret_cast<uint16_t*>(d_slots + cache_off) : nullptr;
+    a.gcache_stride = pl.gcache_stride;
     a.ghdr = pl.walker_ctas ? d_ghdr : nullptr;
     a.split = pl.walker_ctas ? 1 : 0;
     a.producer_ctas = pl.ctas - pl.walker_ctas;
@@ -410,11 +462,14 @@ int Ctx::launch_device(const cmc_params& p, const uint32_t* d_key_in, uint32_t f
 
 // Estimated AES-block cost of one trial of a job (map build + seeds), used to
 // order a batch heaviest first.
-static double job_cost(const Job& j) {
+double job_cost(const Job& j) {
     const double c = std::ldexp(1.0, 2 * int(j.half_bits)) / double(j.domain);
     const double direct = double(j.pnum) * j.k * 8.0 * c;
-    const double cache = 8.0 * std::ldexp(1.0, int(j.half_bits)) + direct / 64.0;
-    return 2.0 + (j.method == kMethodCache ? cache : direct) + 0.1 * j.pnum;
+    const double build = 8.0 * std::ldexp(1.0, int(j.half_bits));
+    const double map = j.method == kMethodCache    ? build + direct / 64.0
+                       : j.method == kMethodGCache ? build + direct * 0.3
+                                                   : direct;
+    return 2.0 + map + 0.1 * j.pnum;
 }
 
 std::string Ctx::mix_key(const cmc_job* in, uint32_t n) const {
@@ -555,13 +610,13 @@ int Ctx::autotune(const cmc_job* in, uint32_t n, uint32_t sample_div) {
     uint64_t total = 0;
     if ((rc = prepare_jobs(in, n, sample_div ? sample_div : 64, jobs, order, total))) return rc;
     cudaStream_t st = user_stream ? user_stream : stream;
-    bool any_h_small = false;
-    for (const Job& j : jobs) any_h_small = any_h_small || j.half_bits <= 12;
+    bool any_cached = false;  // does the automatic choice use a round cache anywhere?
+    for (const Job& j : jobs) any_cached = any_cached || j.method != kMethodDirect;
     std::vector<TunedPlan> cands;
     for (int iso : {0, 1})
         for (uint32_t wg : {1u, 2u, 4u, 6u})
             for (int method : {-1, 0}) {
-                if (method == 0 && !any_h_small) continue;  // auto already picks direct
+                if (method == 0 && !any_cached) continue;  // auto already picks direct
                 cands.push_back(TunedPlan{wg, iso, method});
             }
     if ((rc = grow(d_job_failed, job_failed_cap, n, "job counters"))) return rc;
@@ -678,7 +733,7 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     if (n == "warps_per_group" && value >= 0 && value <= 15) c->force_wg = uint32_t(value);
     else if (n == "groups" && value >= 0 && value <= cmc::kMaxGroups) c->force_ng = uint32_t(value);
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
-    else if (n == "method" && value >= -1 && value <= 1) c->force_method = int(value);
+    else if (n == "method" && value >= -1 && value <= 2) c->force_method = int(value);
     else if (n == "walkers" && value >= 0 && value <= 4) c->force_walkers = uint32_t(value);
     else if (n == "isolate_walkers" && value >= -1 && value <= 1) c->force_isolate = int(value);
     else if (n == "walker_ctas" && value >= -1 && value < c->sms) c->force_walker_ctas = int(value);

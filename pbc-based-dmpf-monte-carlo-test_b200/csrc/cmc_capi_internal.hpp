@@ -20,7 +20,14 @@ struct Plan {
     uint32_t slot_stride = 0, bins_bytes = 0, group_bytes = 0;
     uint32_t group_off = 0, slots_off = 0, smem_bytes = 0, threads = 0, ctas = 0;
     int variant = 0;  // 0: u16 map/bins, 1: u32 map/bins, 2: u32 + 64-bit PRP domain
+    uint64_t gslot_bytes = 0;     // global walk slots (0: slots in shared memory)
+    uint32_t gcache_stride = 0;   // u16 entries per group's global round cache
+    uint64_t gcache_bytes = 0;    // all groups' global round caches
 };
+
+uint32_t choose_method(uint32_t h, uint64_t domain, double candidates, int force, bool may_allocate);
+// Estimated cost of one trial in AES-block equivalents (seeds, map, 0.1 t for the walk).
+double job_cost(const Job& j);
 
 // Planner options chosen by the autotuner for one mix of parameter sets.
 struct TunedPlan {
@@ -62,7 +69,8 @@ struct Ctx {
     uint32_t max_slots_per_group = 8;
     int force_walker_ctas = -1;  // -1 auto, 0 in-SM walker, N split engine
     int force_isolate = -1;      // -1 auto, 0 contiguous warp roles, 1 isolated walkers
-    int force_method = -1;  // -1 auto, 0 direct, 1 cache
+    int force_method = -1;  // -1 auto, 0 direct, 1 cache (shared if h <= 12, else global), 2 global cache
+    bool may_allocate = true;  // false: no global round cache, global slots only if unavoidable
     uint32_t spin_limit = 1u << 26;
 
     ~Ctx();

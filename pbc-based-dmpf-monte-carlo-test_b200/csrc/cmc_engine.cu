@@ -5,7 +5,8 @@
 //     a global work counter, derives the trial's PRP key and walk seed
 //     (cuckoo_bench.cu:226-238), and evaluates the bucket of every (item,
 //     copy) pair -- the map -- either by direct 8-round AES Feistel passes or
-//     from an 8*2^h round cache it builds in shared memory first
+//     from an 8*2^h round cache it builds first, in shared memory (h <= 12) or
+//     in an L2-resident global buffer of its own (h <= 16)
 //     (gpu_shared.cuh:70-91 is the reference's warp-per-trial version).  The
 //     map and an empty table go into a slot.
 //   * one walker warp.  Lane s owns slot s and runs the serial cuckoo
@@ -50,6 +51,7 @@ struct CtaShared {
     SlotHeader slot_hdr[kMaxSlots];
     uint32_t groups_done;
 };
+static_assert(sizeof(CtaShared) <= kCtaSharedBytes, "the planner reserves kCtaSharedBytes");
 
 constexpr uint32_t kCtaSharedOff = kTableBytes;
 
@@ -183,7 +185,10 @@ __device__ __forceinline__ void build_map_direct(const Lanes& L, const Job& J, G
     }
 }
 
-template <typename MapT>
+// Candidates from a round cache (shared or global memory): 8 dependent
+// lookups per Feistel evaluation.  CH independent candidates per lane keep CH
+// lookup chains in flight, which hides the latency of an L2-resident cache.
+template <typename MapT, int CH>
 __device__ __forceinline__ void build_map_cache(const Job& J, GroupHeader* gh,
                                                 const uint16_t* cache, MapT* map,
                                                 uint32_t lane) {
@@ -192,39 +197,83 @@ __device__ __forceinline__ void build_map_cache(const Job& J, GroupHeader* gh,
     const uint32_t domain_m1 = (uint32_t)(J.domain - 1);
     const bool sequential = J.input_mode == 0;
     const uint64_t shift = gh->shift, step = gh->step, range_mask = J.range_mask;
-    uint32_t c = claim(&gh->cand_next, true, lane);
-    bool has = c < ncand;
-    uint32_t l = 0, r = 0;
-    auto start = [&](uint32_t cand) {
-        const uint32_t o = cand / k, j = cand - o * k;
+    uint32_t c[CH], l[CH], r[CH];
+    bool has[CH];
+    auto start = [&](int i) {
+        const uint32_t o = c[i] / k, j = c[i] - o * k;
         const uint64_t e = sequential ? (uint64_t)o : (shift + (uint64_t)o * step) & range_mask;
         const uint32_t y = (uint32_t)(e * k + j);
-        l = y >> h;
-        r = y & mask;
+        l[i] = y >> h;
+        r[i] = y & mask;
     };
-    if (has) start(c);
-    while (__any_sync(kFull, has)) {
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+        c[i] = claim(&gh->cand_next, true, lane);
+        has[i] = c[i] < ncand;
+        l[i] = r[i] = 0;  // idle chains keep in-range indices
+        if (has[i]) start(i);
+        any |= has[i];
+    }
+    while (__any_sync(kFull, any)) {
 #pragma unroll
         for (uint32_t rr = 0; rr < 8; ++rr) {
-            const uint32_t f = cache[(rr << h) | r];
-            const uint32_t nr = l ^ f;
-            l = r;
-            r = nr;
+#pragma unroll
+            for (int i = 0; i < CH; ++i) {
+                const uint32_t f = cache[(rr << h) | r[i]];
+                const uint32_t nr = l[i] ^ f;
+                l[i] = r[i];
+                r[i] = nr;
+            }
         }
-        const uint32_t y = (l << h) | r;
-        const bool done = has && y <= domain_m1;
-        if (done) {
-            map[c] = (MapT)div_width(y, (uint32_t)J.width, J.width_magic);
-        } else if (has) {
-            l = y >> h;
-            r = y & mask;
+        any = false;
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+            const uint32_t y = (l[i] << h) | r[i];
+            const bool done = has[i] && y <= domain_m1;
+            if (done) {
+                map[c[i]] = (MapT)div_width(y, (uint32_t)J.width, J.width_magic);
+            } else if (has[i]) {
+                l[i] = y >> h;
+                r[i] = y & mask;
+            }
+            const uint32_t nc = claim(&gh->cand_next, done, lane);
+            if (done) {
+                c[i] = nc;
+                has[i] = c[i] < ncand;
+                if (has[i]) start(i);
+            }
+            any |= has[i];
         }
-        const uint32_t nc = claim(&gh->cand_next, done, lane);
-        if (done) {
-            c = nc;
-            has = c < ncand;
-            if (has) start(c);
-        }
+    }
+}
+
+// Round cache: entry (r, R) = F_r(R) & mask for the 8 rounds and every h-bit
+// R, 8 * 2^h AES blocks.  Two independent blocks per iteration: their unrolled
+// round chains interleave, doubling the ILP of each warp.
+__device__ __forceinline__ void fill_round_cache(const Lanes& L, const PrpKey& key,
+                                                 const GroupHeader* gh, uint16_t* cache,
+                                                 uint32_t h, uint32_t m, uint32_t gt,
+                                                 uint32_t gthreads) {
+    const uint32_t entries = 8u << h;
+    uint32_t e = gt;
+    for (; e + gthreads < entries; e += 2 * gthreads) {
+        const uint32_t e2 = e + gthreads;
+        const uint32_t r1a = e >> h, r1b = e2 >> h;
+        const uint4 ca = *reinterpret_cast<const uint4*>(&gh->r1[r1a][0]);
+        const uint4 cb = *reinterpret_cast<const uint4*>(&gh->r1[r1b][0]);
+        const Round1 rca{ca.x, ca.y, ca.z, ca.w, gh->r1[r1a][4]};
+        const Round1 rcb{cb.x, cb.y, cb.z, cb.w, gh->r1[r1b][4]};
+        const uint32_t fa = prp_f(L, key, rca, e & m);
+        const uint32_t fb = prp_f(L, key, rcb, e2 & m);
+        cache[e] = (uint16_t)(fa & m);
+        cache[e2] = (uint16_t)(fb & m);
+    }
+    if (e < entries) {
+        const uint32_t rr = e >> h;
+        const uint4 c4 = *reinterpret_cast<const uint4*>(&gh->r1[rr][0]);
+        const Round1 rc{c4.x, c4.y, c4.z, c4.w, gh->r1[rr][4]};
+        cache[e] = (uint16_t)(prp_f(L, key, rc, e & m) & m);
     }
 }
 
@@ -330,31 +379,20 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         }
         PrpKey key;
         if constexpr (!WIDE) prp_key_from_schedule(gh->rk, key);
-        if (!WIDE && J.method == kMethodCache) {
-            const uint32_t h = J.half_bits, entries = 8u << h, m = (uint32_t)J.mask;
-            // Two independent blocks per iteration: their unrolled round
-            // chains interleave, doubling the ILP of each warp.
-            uint32_t e = gt;
-            for (; e + gthreads < entries; e += 2 * gthreads) {
-                const uint32_t e2 = e + gthreads;
-                const uint32_t r1a = e >> h, r1b = e2 >> h;
-                const uint4 ca = *reinterpret_cast<const uint4*>(&gh->r1[r1a][0]);
-                const uint4 cb = *reinterpret_cast<const uint4*>(&gh->r1[r1b][0]);
-                const Round1 rca{ca.x, ca.y, ca.z, ca.w, gh->r1[r1a][4]};
-                const Round1 rcb{cb.x, cb.y, cb.z, cb.w, gh->r1[r1b][4]};
-                const uint32_t fa = prp_f(L, key, rca, e & m);
-                const uint32_t fb = prp_f(L, key, rcb, e2 & m);
-                cache[e] = (uint16_t)(fa & m);
-                cache[e2] = (uint16_t)(fb & m);
-            }
-            if (e < entries) {
-                const uint32_t rr = e >> h;
-                const uint4 c4 = *reinterpret_cast<const uint4*>(&gh->r1[rr][0]);
-                const Round1 rc{c4.x, c4.y, c4.z, c4.w, gh->r1[rr][4]};
-                cache[e] = (uint16_t)(prp_f(L, key, rc, e & m) & m);
-            }
+        // A job uses a round cache only if this launch provides room for it
+        // (a descriptor made under other options falls back to direct passes).
+        const uint32_t cache_entries = 8u << J.half_bits;
+        if (!WIDE && J.method == kMethodCache &&
+            sizeof(GroupHeader) + 2 * cache_entries <= a.group_bytes) {
+            fill_round_cache(L, key, gh, cache, J.half_bits, (uint32_t)J.mask, gt, gthreads);
             group_sync(g, gthreads);
-            build_map_cache<MapT>(J, gh, cache, map, lane);
+            build_map_cache<MapT, 1>(J, gh, cache, map, lane);
+        } else if (!WIDE && J.method == kMethodGCache && a.gcache != nullptr &&
+                   cache_entries <= a.gcache_stride) {
+            uint16_t* gc = a.gcache + (size_t)(blockIdx.x * a.ng + g) * a.gcache_stride;
+            fill_round_cache(L, key, gh, gc, J.half_bits, (uint32_t)J.mask, gt, gthreads);
+            group_sync(g, gthreads);  // orders the group's global writes before its reads
+            build_map_cache<MapT, 2>(J, gh, gc, map, lane);
         } else {
             build_map_direct<MapT, WIDE>(L, J, gh, key, map, lane);
         }
@@ -778,7 +816,7 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
         }
     }
     CtaShared* cs = reinterpret_cast<CtaShared*>(smem + kCtaSharedOff);
-    if (threadIdx.x < kMaxSlots) cs->slot_state[threadIdx.x] = kSlotFree;
+    for (uint32_t i = threadIdx.x; i < kMaxSlots; i += blockDim.x) cs->slot_state[i] = kSlotFree;
     if (threadIdx.x == 0) cs->groups_done = 0;
     __syncthreads();
     // Warp roles.  Warp w issues from SM sub-partition w % 4.  With

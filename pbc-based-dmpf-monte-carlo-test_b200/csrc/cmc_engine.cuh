@@ -7,12 +7,14 @@ namespace cmc {
 
 constexpr uint32_t kMethodDirect = 0;  // candidates by 8-round AES Feistel passes
 constexpr uint32_t kMethodCache = 1;   // 8*2^h round cache in shared memory, then lookups
+constexpr uint32_t kMethodGCache = 2;  // the same round cache in global memory (L2), h <= 16
 
 constexpr uint32_t kSlotFree = 0;
 constexpr uint32_t kSlotReady = 1;
 constexpr uint32_t kSlotFilling = 2;
 
-constexpr uint32_t kMaxSlots = 32;  // one walker lane per slot
+constexpr uint32_t kMaxSlots = 128;  // one walker lane per slot, up to 4 walker warps
+constexpr uint32_t kCtaSharedBytes = 4864;  // slot states and headers after the T-table
 constexpr uint32_t kEngineTableBytes = 65536;  // replicated T-table at shared offset 0
 constexpr uint32_t kMaxGroups = 14; // named barriers 1..14
 
@@ -80,6 +82,10 @@ struct EngineArgs {
     uint32_t group_off;                 // smem offset of group 0
     uint32_t slots_off;                 // smem offset of slot 0 (smem slots)
     uint32_t spin_limit;                // bounded waits (polls of ~0.5 us)
+    // global round caches (kMethodGCache jobs): group (cta, g) owns entries
+    // [(cta * ng + g) * gcache_stride, +8 << h)
+    uint16_t* gcache;
+    uint32_t gcache_stride;
 };
 
 // Serving: device-resident state of one admitted job.  `next` is the job's

@@ -127,6 +127,7 @@ int setup(int device, DeviceState*& out) {
     Ctx* planner = new (g_planner_storage[device]) Ctx();  // never destroyed: lives with the scratch
     planner->sms = sms;
     planner->smem_optin = size_t(optin);
+    planner->may_allocate = false;  // global round caches and slots would need an allocation
     st.scratch = static_cast<unsigned char*>(scratch);
     st.t0 = static_cast<uint32_t*>(t0);
     st.planner = planner;

@@ -8,8 +8,9 @@
 // (`cmc_server_step`):
 //   1. admits queued jobs while their slot memory fits the device-memory budget;
 //   2. picks one size class (jobs whose walk slots fit in shared memory, or
-//      not) and grants its jobs trials: half of the step's work in arrival
-//      order, so no job starves, half shortest remaining work first;
+//      not) and grants its jobs trials: most of the step's work (95% by
+//      default) in arrival order, so no job starves and the tail stays that
+//      of plain per-job launches, the rest shortest remaining work first;
 //   3. the scheduler kernel turns the grants into the engine's job table on the
 //      device -- clamping at batch ends, deriving a batch key with device AES
 //      when a job enters a new batch, advancing the RNG counters, prefix-summing
@@ -119,7 +120,9 @@ __global__ void __launch_bounds__(256) serve_schedule(ServeState* __restrict__ s
 struct HostJob {
     uint32_t id = 0;
     cmc_params params{};
-    uint64_t seed = 0, budget = 0, next = 0;
+    uint64_t seed = 0, budget = 0;
+    uint64_t next = 0;       // trials granted (issued to the device)
+    uint64_t processed = 0;  // trials whose results the host has read back
     int state = 0;  // 0 queued, 1 active, 2 done
     uint32_t slot = 0;
     double cost = 1;  // estimated AES blocks per trial
@@ -136,26 +139,53 @@ struct HostJob {
 
 }  // namespace
 
+// One iteration in flight: its stream, device buffers, pinned read-back
+// buffers and the grants it carries.  Two of them alternate, so the host
+// plans and issues iteration i+1 while iteration i runs, and the next engine's
+// CTAs start on the SMs the previous engine's tail frees.
+struct StepBuf {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t sched_done = nullptr;  // job states advanced by this iteration's scheduler
+    cudaEvent_t done = nullptr;        // everything of this iteration finished
+    cudaEvent_t e0 = nullptr, e1 = nullptr;  // around the engine launch (timing)
+    uint64_t trials = 0;               // trials this iteration carries
+    Grant* d_grants = nullptr;
+    Job* d_table = nullptr;
+    GrantInfo* d_info = nullptr;
+    unsigned long long* d_total = nullptr;
+    Ctrl* d_ctrl = nullptr;
+    uint32_t* d_bits = nullptr;
+    uint32_t* d_list = nullptr;  // failures of the iteration (+ count)
+    char* d_pool = nullptr;      // global walk slots and round caches
+    uint64_t pool_bytes = 0;
+    Grant* h_grants = nullptr;   // pinned
+    GrantInfo* h_info = nullptr; // pinned
+    uint32_t* h_count = nullptr; // pinned
+    Ctrl* h_ctrl = nullptr;      // pinned
+    bool busy = false;
+    std::vector<uint32_t> grant_jobs;  // job id of each grant
+};
+
 struct Server {
     Ctx* ctx = nullptr;
     uint32_t max_jobs = 0, bt = 20;
     uint64_t mem_budget = 0, max_iter_trials = 0, iteration = 0;
     ServeState* d_states = nullptr;
-    Grant* d_grants = nullptr;
-    Job* d_table = nullptr;
-    GrantInfo* d_info = nullptr;
-    unsigned long long* d_total = nullptr;
+    ServeState* h_stage = nullptr;  // pinned staging of admitted job states
     unsigned long long* d_failed = nullptr;
     unsigned long long* d_done = nullptr;
-    uint32_t* d_bits = nullptr;
-    uint32_t* d_list = nullptr;  // failures of one iteration (+ count)
-    char* d_slots = nullptr;
-    size_t slots_bytes = 0;
+    StepBuf bufs[2];
+    uint32_t cur = 0;       // buffer of the next iteration
+    bool sched_seen = false;  // some iteration's scheduler has been issued
+    cudaEvent_t origin = nullptr;  // time origin of the engine intervals
+    cmc_server_stats stats{};
+    double last_end_ms = -1;     // end of the previous engine interval (from origin)
+    double first_start_ms = 0;
     std::vector<HostJob> jobs;
     std::deque<uint32_t> queue;
     std::vector<uint32_t> free_slots;
     uint64_t fixed_bytes = 0;
-    double fifo_share = 0.5;  // part of each step's work granted in arrival order
+    double fifo_share = 0.95;  // part of each step's work granted in arrival order
     std::string err;
 
     int fail(int code, const std::string& m) {
@@ -167,16 +197,33 @@ struct Server {
         return fail(CMC_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
     }
     ~Server() {
+        for (StepBuf& b : bufs) {
+            if (b.stream) cudaStreamSynchronize(b.stream);
+        }
+        for (StepBuf& b : bufs) {
+            cudaFree(b.d_grants);
+            cudaFree(b.d_table);
+            cudaFree(b.d_info);
+            cudaFree(b.d_total);
+            cudaFree(b.d_ctrl);
+            cudaFree(b.d_bits);
+            cudaFree(b.d_list);
+            cudaFree(b.d_pool);
+            cudaFreeHost(b.h_grants);
+            cudaFreeHost(b.h_info);
+            cudaFreeHost(b.h_count);
+            cudaFreeHost(b.h_ctrl);
+            if (b.sched_done) cudaEventDestroy(b.sched_done);
+            if (b.done) cudaEventDestroy(b.done);
+            if (b.e0) cudaEventDestroy(b.e0);
+            if (b.e1) cudaEventDestroy(b.e1);
+            if (b.stream) cudaStreamDestroy(b.stream);
+        }
+        if (origin) cudaEventDestroy(origin);
         cudaFree(d_states);
-        cudaFree(d_grants);
-        cudaFree(d_table);
-        cudaFree(d_info);
-        cudaFree(d_total);
+        cudaFreeHost(h_stage);
         cudaFree(d_failed);
         cudaFree(d_done);
-        cudaFree(d_bits);
-        cudaFree(d_list);
-        cudaFree(d_slots);
     }
 
     int init(Ctx* c, uint32_t mj, uint64_t budget, uint32_t batch_bits, uint64_t iter_trials) {
@@ -194,42 +241,69 @@ struct Server {
             }
             return CMC_OK;
         };
+        auto host = [&](void** p, size_t bytes, const char* what) {
+            if (cudaHostAlloc(p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(CMC_ENOMEM, std::string("cudaHostAlloc for ") + what);
+            }
+            return CMC_OK;
+        };
         const size_t words = (max_iter_trials + 31) / 32;
         if ((rc = alloc((void**)&d_states, sizeof(ServeState) * mj, "job states"))) return rc;
-        if ((rc = alloc((void**)&d_grants, sizeof(Grant) * mj, "grants"))) return rc;
-        if ((rc = alloc((void**)&d_table, sizeof(Job) * mj, "job table"))) return rc;
-        if ((rc = alloc((void**)&d_info, sizeof(GrantInfo) * mj, "grant info"))) return rc;
-        if ((rc = alloc((void**)&d_total, 8, "total"))) return rc;
+        if ((rc = host((void**)&h_stage, sizeof(ServeState) * mj, "job state staging"))) return rc;
         if ((rc = alloc((void**)&d_failed, 8 * mj, "failure counters"))) return rc;
         if ((rc = alloc((void**)&d_done, 8 * mj, "trial counters"))) return rc;
-        if ((rc = alloc((void**)&d_bits, words * 4, "failure bitmap"))) return rc;
-        if ((rc = alloc((void**)&d_list, (max_iter_trials + 1) * 4, "failure list"))) return rc;
-        fixed_bytes = (sizeof(ServeState) + sizeof(Grant) + sizeof(Job) + sizeof(GrantInfo) + 16) * mj +
-                      words * 4 + (max_iter_trials + 1) * 4 + 8;
+        for (StepBuf& b : bufs) {
+            if ((rc = cuda(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking), "stream"))) return rc;
+            if ((rc = cuda(cudaEventCreateWithFlags(&b.sched_done, cudaEventDisableTiming), "event"))) return rc;
+            if ((rc = cuda(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming), "event"))) return rc;
+            if ((rc = cuda(cudaEventCreate(&b.e0), "event"))) return rc;
+            if ((rc = cuda(cudaEventCreate(&b.e1), "event"))) return rc;
+            if ((rc = alloc((void**)&b.d_grants, sizeof(Grant) * mj, "grants"))) return rc;
+            if ((rc = alloc((void**)&b.d_table, sizeof(Job) * mj, "job table"))) return rc;
+            if ((rc = alloc((void**)&b.d_info, sizeof(GrantInfo) * mj, "grant info"))) return rc;
+            if ((rc = alloc((void**)&b.d_total, 8, "total"))) return rc;
+            if ((rc = alloc((void**)&b.d_ctrl, sizeof(Ctrl), "control block"))) return rc;
+            if ((rc = alloc((void**)&b.d_bits, words * 4, "failure bitmap"))) return rc;
+            if ((rc = alloc((void**)&b.d_list, (max_iter_trials + 1) * 4, "failure list"))) return rc;
+            if ((rc = host((void**)&b.h_grants, sizeof(Grant) * mj, "grants"))) return rc;
+            if ((rc = host((void**)&b.h_info, sizeof(GrantInfo) * mj, "grant info"))) return rc;
+            if ((rc = host((void**)&b.h_count, 4, "count"))) return rc;
+            if ((rc = host((void**)&b.h_ctrl, sizeof(Ctrl), "control block"))) return rc;
+        }
+        fixed_bytes = (sizeof(ServeState) + 16) * mj +
+                      2 * ((sizeof(Grant) + sizeof(Job) + sizeof(GrantInfo)) * mj + words * 4 +
+                           (max_iter_trials + 1) * 4 + 8 + sizeof(Ctrl));
         if (fixed_bytes > mem_budget) return fail(CMC_ENOMEM, "device-memory budget below the server's fixed state");
         for (uint32_t s = mj; s-- > 0;) free_slots.push_back(s);
-        if ((rc = cuda(cudaMemsetAsync(d_failed, 0, 8 * mj, ctx->stream), "memset"))) return rc;
-        if ((rc = cuda(cudaMemsetAsync(d_done, 0, 8 * mj, ctx->stream), "memset"))) return rc;
+        if ((rc = cuda(cudaMemsetAsync(d_failed, 0, 8 * mj, bufs[0].stream), "memset"))) return rc;
+        if ((rc = cuda(cudaMemsetAsync(d_done, 0, 8 * mj, bufs[0].stream), "memset"))) return rc;
+        if ((rc = cuda(cudaEventCreate(&origin), "event"))) return rc;
+        if ((rc = cuda(cudaEventRecord(origin, bufs[0].stream), "event"))) return rc;
+        if ((rc = cuda(cudaStreamSynchronize(bufs[0].stream), "init sync"))) return rc;
         return cuda(cudaFuncSetAttribute((const void*)serve_schedule,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kTableBytes),
                     "scheduler attribute");
     }
 
-    // Plan for a set of active parameter sets; returns the global slot pool
-    // bytes the plan needs (0 for shared-memory slots).
-    int plan_for(const std::vector<uint32_t>& ids, Plan& pl, std::vector<Job>& shapes, uint64_t& pool) {
+    // Plan for a set of active parameter sets; returns the global pool bytes
+    // the plan needs: walk slots (0 for shared-memory slots), then round caches.
+    int plan_for(const std::vector<uint32_t>& ids, Plan& pl, std::vector<Job>& shapes, uint64_t& pool,
+                 const std::vector<uint32_t>* weights = nullptr) {
         shapes.clear();
-        for (uint32_t id : ids) {
+        for (size_t i = 0; i < ids.size(); ++i) {
             Job j;
-            int rc = ctx->make_job(jobs[id].params, 0, 1, 0, j);
+            int rc = ctx->make_job(jobs[ids[i]].params, 0, weights ? (*weights)[i] : 1, 0, j);
             if (rc) return fail(rc, ctx->err);
             shapes.push_back(j);
         }
         int rc = ctx->plan(shapes, pl);
         if (rc) return fail(rc, ctx->err);
-        pool = pl.slots_smem ? 0 : uint64_t(pl.ctas) * pl.ns * pl.slot_stride;
+        pool = cache_offset(pl) + pl.gcache_bytes;
         return CMC_OK;
     }
+
+    static uint64_t cache_offset(const Plan& pl) { return (pl.gslot_bytes + 255) / 256 * 256; }
 
     std::vector<uint32_t> active_ids() const {
         std::vector<uint32_t> v;
@@ -257,9 +331,7 @@ struct Server {
         while ((1ULL << et) < trials) ++et;
         j.bt = std::min(bt, std::max(et, 1u));
         j.budget = ((trials + (1ULL << j.bt) - 1) >> j.bt) << j.bt;
-        const double c = std::ldexp(1.0, 2 * int(p.half_bits)) / double(p.domain);
-        j.cost = 2.0 + std::min(8.0 * std::ldexp(1.0, int(p.half_bits)), 8.0 * p.k * p.pnum * c) +
-                 0.3 * p.pnum;
+        j.cost = job_cost(probe) + 0.2 * p.pnum;
         {
             // size class: do this table's walk slots fit in shared memory?
             std::vector<Job> one(1);
@@ -267,9 +339,9 @@ struct Server {
             Plan pl;
             if ((rc = ctx->plan(one, pl))) return fail(rc, ctx->err);
             j.global_slots = pl.slots_smem ? 0 : 1;
-            // a trial's walk is ~2.4 t probes of ~300 (shared) or ~1300 (global)
+            // a trial's walk is ~2.4 t probes of ~300 (shared) or ~3000 (global)
             // cycles; expressed in blocks of GPU throughput (~4e10 blocks/s at 2 GHz)
-            const double walk_cycles = 2.4 * p.pnum * (j.global_slots ? 1300.0 : 300.0);
+            const double walk_cycles = 2.4 * p.pnum * (j.global_slots ? 3000.0 : 300.0);
             j.latency_blocks = walk_cycles / 2.0e9 * 4.0e10;
         }
         if (journal_dir && *journal_dir) {
@@ -293,6 +365,7 @@ struct Server {
                 uint64_t b = 0;
                 while (b < done.size() && done[b]) ++b;
                 j.next = std::min<uint64_t>(j.budget, b << j.bt);
+                j.processed = j.next;
                 j.failed = c0.failed.load();  // committed failures of the prefix
                 j.journal.reset(new Journal(o, p, 0));
             } catch (const std::exception& e) {
@@ -305,7 +378,10 @@ struct Server {
         return CMC_OK;
     }
 
-    int admit() {
+    // Admission on the stream of the next iteration: job state from pinned
+    // staging (slot s's staging entry is rewritten only after the job in slot s
+    // retired, i.e. after its upload was long consumed) and zeroed counters.
+    int admit(cudaStream_t st) {
         while (!queue.empty() && !free_slots.empty()) {
             const uint32_t id = queue.front();
             HostJob& j = jobs[id];
@@ -321,7 +397,7 @@ struct Server {
             uint64_t pool = 0;
             int rc = plan_for(ids, pl, shapes, pool);
             if (rc) return rc;
-            if (fixed_bytes + pool > mem_budget) {
+            if (fixed_bytes + 2 * pool > mem_budget) {  // two iterations in flight
                 if (ids.size() == 1)
                     return fail(CMC_ENOMEM, "job " + std::to_string(id) +
                                                 " alone needs more device memory than the budget");
@@ -332,36 +408,70 @@ struct Server {
             free_slots.pop_back();
             j.state = 1;
             j.admitted_at = iteration;
-            ServeState st{};
-            rc = ctx->make_job(j.params, 0, 1, 0, st.job);
+            ServeState state{};
+            rc = ctx->make_job(j.params, 0, 1, 0, state.job);
             if (rc) return fail(rc, ctx->err);
-            st.seed = j.seed;
-            st.next = j.next;
-            st.budget = j.budget;
-            st.key_batch = ~0ULL;
-            st.bt = j.bt;
-            st.active = 1;
-            const uint64_t zero = 0;
-            if ((rc = cuda(cudaMemcpyAsync(&d_states[j.slot], &st, sizeof st, cudaMemcpyHostToDevice,
-                                           ctx->stream), "upload job state")))
+            state.seed = j.seed;
+            state.next = j.next;
+            state.budget = j.budget;
+            state.key_batch = ~0ULL;
+            state.bt = j.bt;
+            state.active = 1;
+            h_stage[j.slot] = state;
+            if ((rc = cuda(cudaMemcpyAsync(&d_states[j.slot], &h_stage[j.slot], sizeof state,
+                                           cudaMemcpyHostToDevice, st), "upload job state")))
                 return rc;
-            if ((rc = cuda(cudaMemcpyAsync(&d_failed[j.slot], &zero, 8, cudaMemcpyHostToDevice, ctx->stream),
-                           "reset counter")))
-                return rc;
-            if ((rc = cuda(cudaMemcpyAsync(&d_done[j.slot], &zero, 8, cudaMemcpyHostToDevice, ctx->stream),
-                           "reset counter")))
-                return rc;
-            if ((rc = cuda(cudaStreamSynchronize(ctx->stream), "admit sync"))) return rc;
+            if ((rc = cuda(cudaMemsetAsync(&d_failed[j.slot], 0, 8, st), "reset counter"))) return rc;
+            if ((rc = cuda(cudaMemsetAsync(&d_done[j.slot], 0, 8, st), "reset counter"))) return rc;
         }
         return CMC_OK;
     }
 
+    // One iteration: admit, plan and issue this iteration's grants, then read
+    // back the previous iteration's results (which ran meanwhile) and commit
+    // them.  Jobs finish in the call after their last trials were issued.
     int step(uint64_t work_blocks, uint32_t* finished, uint32_t cap, uint32_t* nfinished) {
         if (nfinished) *nfinished = 0;
         int rc = cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
         if (rc) return rc;
-        if ((rc = admit())) return rc;
-        std::vector<uint32_t> all = active_ids();
+        StepBuf& b = bufs[cur];
+        StepBuf& prev = bufs[cur ^ 1];
+        if (b.busy && (rc = process(b, finished, cap, nfinished))) return rc;  // not reached in order
+        if ((rc = admit(b.stream))) return rc;
+        std::vector<Grant> grants;
+        std::vector<uint32_t> grant_jobs;
+        if ((rc = plan_grants(work_blocks, grants, grant_jobs))) return rc;
+        if (!grants.empty()) {
+            if ((rc = issue(b, grants, grant_jobs))) return rc;
+            cur ^= 1;
+        }
+        if (prev.busy) {
+            uint32_t n = nfinished ? *nfinished : 0;
+            if ((rc = process(prev, finished ? finished + std::min(n, cap) : nullptr, cap - std::min(n, cap),
+                              &n)))
+                return rc;
+            if (nfinished) *nfinished += n;
+        }
+        return CMC_OK;
+    }
+
+    // Finishes every iteration in flight (used before the server goes away,
+    // so journals hold every batch the device completed).
+    int drain() {
+        for (int i = 0; i < 2; ++i) {
+            StepBuf& b = bufs[(cur + i) & 1];  // oldest first
+            if (b.busy) {
+                int rc = process(b, nullptr, 0, nullptr);
+                if (rc) return rc;
+            }
+        }
+        return CMC_OK;
+    }
+
+    int plan_grants(uint64_t work_blocks, std::vector<Grant>& grants, std::vector<uint32_t>& grant_jobs) {
+        std::vector<uint32_t> all;  // active jobs with trials left to issue
+        for (uint32_t id : active_ids())
+            if (jobs[id].next < jobs[id].budget) all.push_back(id);
         if (all.empty()) return CMC_OK;
         // One size class per step, so the plan keeps shared-memory walk slots
         // whenever the granted tables allow: alternately the class of the
@@ -376,16 +486,22 @@ struct Server {
         std::vector<uint32_t> ids;
         for (uint32_t id : all)
             if (jobs[id].global_slots == cls) ids.push_back(id);
-        // grants: half of the work in arrival order (bounds the tail), the rest
-        // shortest remaining work first (small jobs finish at once); the step
-        // is at least 2.5x the latency of its slowest trial so that trial's
-        // tail is covered
-        std::vector<Grant> grants;
+        // grants: fifo_share of the work in arrival order (bounds the tail),
+        // the rest shortest remaining work first (small jobs finish at once);
+        // the step is at least 2.5x the latency of its slowest trial so that
+        // trial's tail is covered
         std::vector<uint32_t> order = ids;
         std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return remaining(a) < remaining(b); });
         double floor_blocks = 0;
         for (uint32_t id : ids) floor_blocks = std::max(floor_blocks, 2.5 * jobs[id].latency_blocks);
-        work_blocks = std::max<uint64_t>(work_blocks, uint64_t(floor_blocks));
+        // Backlog-adaptive size: an eighth of the class's outstanding work,
+        // between work_blocks and 20x work_blocks.  A light load runs short
+        // iterations (an arrival waits little); a backlog runs long ones
+        // (fewer iteration tails, measured 1.2x throughput at 20x).
+        double backlog = 0;
+        for (uint32_t id : ids) backlog += remaining(id);
+        const double adaptive = std::min(backlog / 8.0, 20.0 * double(work_blocks));
+        work_blocks = std::max<uint64_t>({work_blocks, uint64_t(floor_blocks), uint64_t(adaptive)});
         // shares per job (trials), then one grant per job
         std::vector<uint64_t> share(ids.size(), 0);
         std::vector<uint32_t> pos(jobs.size(), 0);
@@ -421,49 +537,77 @@ struct Server {
             if (left <= 0 || trials_left == 0) break;
             give(id, left);
         }
-        for (uint32_t i = 0; i < ids.size(); ++i) {
-            if (share[i] == 0) continue;
+        // the table runs heaviest trials first (as cmc_run_jobs does), so the
+        // iteration ends on short trials instead of on the longest walks
+        std::vector<uint32_t> heavy;
+        for (uint32_t i = 0; i < ids.size(); ++i)
+            if (share[i] > 0) heavy.push_back(i);
+        std::stable_sort(heavy.begin(), heavy.end(),
+                         [&](uint32_t a, uint32_t b) { return jobs[ids[a]].cost > jobs[ids[b]].cost; });
+        for (uint32_t i : heavy) {
             HostJob& j = jobs[ids[i]];
             grants.push_back(Grant{j.slot, uint32_t(share[i])});
+            grant_jobs.push_back(ids[i]);
             j.next += share[i];
         }
-        if (grants.empty()) return CMC_OK;
-        cudaStream_t st = ctx->stream;
-        if ((rc = cuda(cudaMemcpyAsync(d_grants, grants.data(), grants.size() * sizeof(Grant),
-                                       cudaMemcpyHostToDevice, st), "upload grants")))
-            return rc;
-        serve_schedule<<<1, 256, kTableBytes, st>>>(d_states, d_grants, uint32_t(grants.size()), ctx->d_t0,
-                                                    d_table, d_info, d_total);
-        if ((rc = cuda(cudaGetLastError(), "scheduler launch"))) return rc;
-        // engine over the table the scheduler wrote
+        return CMC_OK;
+    }
+
+    // Queue one iteration on b's stream: grants -> scheduler -> engine ->
+    // compaction -> read-back into pinned memory.
+    int issue(StepBuf& b, const std::vector<Grant>& grants, const std::vector<uint32_t>& grant_jobs) {
+        int rc = CMC_OK;
+        cudaStream_t st = b.stream;
+        std::vector<uint32_t> weights;  // the plan weighs each shape by its granted trials
+        for (const Grant& g : grants) weights.push_back(g.trials);
         Plan pl;
         std::vector<Job> shapes;
         uint64_t pool = 0;
-        if ((rc = plan_for(ids, pl, shapes, pool))) return rc;
-        if (pool > slots_bytes) {
-            cudaFree(d_slots);
-            d_slots = nullptr;
-            slots_bytes = 0;
-            if (cudaMalloc((void**)&d_slots, pool) != cudaSuccess) {
+        if ((rc = plan_for(grant_jobs, pl, shapes, pool, &weights))) return rc;
+        if (pool > b.pool_bytes) {
+            // grow with headroom (within the budget): each regrowth's cudaFree
+            // waits for the device and drains the pipeline
+            const uint64_t room = mem_budget > fixed_bytes ? (mem_budget - fixed_bytes) / 2 : pool;
+            const uint64_t want = std::max(pool, std::min<uint64_t>(pool + pool / 2, room));
+            cudaFree(b.d_pool);
+            b.d_pool = nullptr;
+            b.pool_bytes = 0;
+            if (cudaMalloc((void**)&b.d_pool, want) != cudaSuccess) {
                 cudaGetLastError();
                 return fail(CMC_ENOMEM, "slot pool");
             }
-            slots_bytes = pool;
+            b.pool_bytes = want;
         }
-        if ((rc = cuda(cudaMemsetAsync(ctx->d_ctrl, 0, sizeof(Ctrl), st), "memset ctrl"))) return rc;
-        if ((rc = cuda(cudaMemsetAsync(d_bits, 0, (max_iter_trials + 31) / 32 * 4, st), "memset bitmap")))
+        std::copy(grants.begin(), grants.end(), b.h_grants);
+        if ((rc = cuda(cudaMemcpyAsync(b.d_grants, b.h_grants, grants.size() * sizeof(Grant),
+                                       cudaMemcpyHostToDevice, st), "upload grants")))
+            return rc;
+        // schedulers run in issue order: each advances the RNG counters the
+        // next one starts from
+        const StepBuf& other = bufs[(&b == &bufs[0]) ? 1 : 0];
+        if (sched_seen && (rc = cuda(cudaStreamWaitEvent(st, other.sched_done, 0), "order schedulers")))
+            return rc;
+        serve_schedule<<<1, 256, kTableBytes, st>>>(d_states, b.d_grants, uint32_t(grants.size()), ctx->d_t0,
+                                                    b.d_table, b.d_info, b.d_total);
+        if ((rc = cuda(cudaGetLastError(), "scheduler launch"))) return rc;
+        if ((rc = cuda(cudaEventRecord(b.sched_done, st), "event"))) return rc;
+        sched_seen = true;
+        if ((rc = cuda(cudaMemsetAsync(b.d_ctrl, 0, sizeof(Ctrl), st), "memset ctrl"))) return rc;
+        if ((rc = cuda(cudaMemsetAsync(b.d_bits, 0, (max_iter_trials + 31) / 32 * 4, st), "memset bitmap")))
             return rc;
         EngineArgs a{};
-        a.jobs = d_table;
+        a.jobs = b.d_table;
         a.njobs = uint32_t(grants.size());
         a.total = 0;
-        a.total_dev = d_total;
+        a.total_dev = b.d_total;
         a.count_by_user = 1;
-        a.ctrl = ctx->d_ctrl;
-        a.fail_bits = d_bits;
+        a.ctrl = b.d_ctrl;
+        a.fail_bits = b.d_bits;
         a.job_failed = d_failed;
         a.job_done = d_done;
-        a.gslots = pl.slots_smem ? nullptr : d_slots;
+        a.gslots = pl.slots_smem ? nullptr : b.d_pool;
+        a.gcache = pl.gcache_bytes ? reinterpret_cast<uint16_t*>(b.d_pool + cache_offset(pl)) : nullptr;
+        a.gcache_stride = pl.gcache_stride;
         a.t0 = ctx->d_t0;
         a.slot_stride = pl.slot_stride;
         a.bins_bytes = pl.bins_bytes;
@@ -484,62 +628,98 @@ struct Server {
                                             int(pl.smem_bytes)), "engine attribute")))
             return rc;
         void* args[] = {&a};
+        if ((rc = cuda(cudaEventRecord(b.e0, st), "event"))) return rc;
         if ((rc = cuda(cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, st),
                        "engine launch")))
             return rc;
-        cmc_compact_failures<<<1, 1024, 0, st>>>(d_bits, 0, 0, d_list, d_list + max_iter_trials,
-                                                 max_iter_trials, d_total);
+        if ((rc = cuda(cudaEventRecord(b.e1, st), "event"))) return rc;
+        cmc_compact_failures<<<1, 1024, 0, st>>>(b.d_bits, 0, 0, b.d_list, b.d_list + max_iter_trials,
+                                                 max_iter_trials, b.d_total);
         if ((rc = cuda(cudaGetLastError(), "compaction launch"))) return rc;
-        std::vector<GrantInfo> info(grants.size());
-        uint32_t nf = 0;
-        if ((rc = cuda(cudaMemcpyAsync(info.data(), d_info, info.size() * sizeof(GrantInfo),
+        if ((rc = cuda(cudaMemcpyAsync(b.h_info, b.d_info, grants.size() * sizeof(GrantInfo),
                                        cudaMemcpyDeviceToHost, st), "read grant info")))
             return rc;
-        if ((rc = cuda(cudaMemcpyAsync(&nf, d_list + max_iter_trials, 4, cudaMemcpyDeviceToHost, st),
+        if ((rc = cuda(cudaMemcpyAsync(b.h_count, b.d_list + max_iter_trials, 4, cudaMemcpyDeviceToHost, st),
                        "read count")))
             return rc;
-        if ((rc = cuda(cudaStreamSynchronize(st), "iteration sync"))) return rc;
-        if ((rc = ctx->check_ctrl())) return fail(rc, ctx->err);
-        ++iteration;
-        std::vector<uint32_t> fl(nf);
-        if (nf && (rc = cuda(cudaMemcpy(fl.data(), d_list, nf * 4ULL, cudaMemcpyDeviceToHost), "read failures")))
+        if ((rc = cuda(cudaMemcpyAsync(b.h_ctrl, b.d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st),
+                       "read ctrl")))
             return rc;
-        // slot -> job
-        std::vector<uint32_t> slot_job(max_jobs, ~0u);
-        for (uint32_t id : ids) slot_job[jobs[id].slot] = id;
+        if ((rc = cuda(cudaEventRecord(b.done, st), "event"))) return rc;
+        b.grant_jobs = grant_jobs;
+        b.trials = 0;
+        for (const Grant& g : grants) b.trials += g.trials;
+        b.busy = true;
+        ++iteration;
+        return CMC_OK;
+    }
+
+    // Wait for b's iteration, map its failures back to (job, batch, offset),
+    // commit completed batches to journals and retire finished jobs.
+    int process(StepBuf& b, uint32_t* finished, uint32_t cap, uint32_t* nfinished) {
+        if (nfinished) *nfinished = 0;
+        b.busy = false;
+        int rc = cuda(cudaEventSynchronize(b.done), "iteration sync");
+        if (rc) return rc;
+        if (b.h_ctrl->error)
+            return fail(-int(b.h_ctrl->error), "device wait gave up (site " + std::to_string(b.h_ctrl->where) +
+                                                   "): results discarded");
+        {
+            float t0 = 0, t1 = 0;
+            if ((rc = cuda(cudaEventElapsedTime(&t0, origin, b.e0), "engine timing"))) return rc;
+            if ((rc = cuda(cudaEventElapsedTime(&t1, origin, b.e1), "engine timing"))) return rc;
+            stats.iterations += 1;
+            stats.trials += b.trials;
+            stats.engine_ms += t1 - t0;
+            // engines of consecutive iterations may overlap: count device time once
+            stats.busy_ms += std::max(0.0, double(t1) - std::max(double(t0), last_end_ms));
+            if (stats.iterations == 1) first_start_ms = t0;
+            last_end_ms = std::max(last_end_ms, double(t1));
+            stats.span_ms = last_end_ms - first_start_ms;
+        }
+        const uint32_t nf = *b.h_count;
+        std::vector<uint32_t> fl(nf);
+        if (nf) {
+            if ((rc = cuda(cudaMemcpyAsync(fl.data(), b.d_list, nf * 4ULL, cudaMemcpyDeviceToHost, b.stream),
+                           "read failures")))
+                return rc;
+            if ((rc = cuda(cudaStreamSynchronize(b.stream), "read failures"))) return rc;
+        }
         // failures of this iteration into their job's pending batch lists
         size_t gi = 0;
-        for (uint32_t g = 0; g < info.size(); ++g) {
-            HostJob& j = jobs[slot_job[info[g].slot]];
+        for (uint32_t g = 0; g < b.grant_jobs.size(); ++g) {
+            const GrantInfo& info = b.h_info[g];
+            HostJob& j = jobs[b.grant_jobs[g]];
             auto& pend = j.pending;
-            if (pend.empty() || pend.back().first != info[g].batch) pend.push_back({info[g].batch, {}});
-            while (gi < fl.size() && fl[gi] < info[g].base + info[g].count) {
-                pend.back().second.push_back(info[g].first + uint32_t(fl[gi] - info[g].base));
+            if (pend.empty() || pend.back().first != info.batch) pend.push_back({info.batch, {}});
+            while (gi < fl.size() && fl[gi] < info.base + info.count) {
+                pend.back().second.push_back(info.first + uint32_t(fl[gi] - info.base));
                 ++j.failed;
                 ++gi;
             }
+            j.processed += info.count;
         }
         // commit finished batches, retire finished jobs
         uint32_t nfin = 0;
-        for (uint32_t id : ids) {
+        for (uint32_t id : b.grant_jobs) {
             HostJob& j = jobs[id];
             const uint64_t per = 1ULL << j.bt;
             while (!j.pending.empty()) {
-                const uint64_t b = j.pending.front().first;
-                const uint64_t end = std::min<uint64_t>((b + 1) << j.bt, j.budget);
-                if (j.next < end) break;  // batch not complete yet
+                const uint64_t bb = j.pending.front().first;
+                const uint64_t end = std::min<uint64_t>((bb + 1) << j.bt, j.budget);
+                if (j.processed < end) break;  // batch not complete yet
                 auto& offs = j.pending.front().second;
                 std::sort(offs.begin(), offs.end());
                 if (j.journal) {
                     try {
-                        j.journal->append(b, uint32_t(std::min<uint64_t>(per, batch_length(j.jopt, b))), offs);
+                        j.journal->append(bb, uint32_t(std::min<uint64_t>(per, batch_length(j.jopt, bb))), offs);
                     } catch (const std::exception& e) {
                         return fail(CMC_EINVAL, std::string("journal: ") + e.what());
                     }
                 }
                 j.pending.erase(j.pending.begin());
             }
-            if (j.next >= j.budget && j.pending.empty()) {
+            if (j.state == 1 && j.processed >= j.budget && j.pending.empty()) {
                 j.state = 2;
                 j.journal.reset();
                 free_slots.push_back(j.slot);
@@ -554,7 +734,7 @@ struct Server {
     int status(uint32_t id, uint64_t* done, uint64_t* failed, int* state) {
         if (id >= jobs.size()) return fail(CMC_EINVAL, "unknown job id");
         HostJob& j = jobs[id];
-        if (done) *done = j.next;
+        if (done) *done = j.processed;
         if (failed) *failed = j.failed;
         if (state) *state = j.state;
         return CMC_OK;
@@ -610,6 +790,12 @@ int cmc_server_policy(cmc_server* server, double fifo_share) {
     return CMC_OK;
 }
 
+int cmc_server_get_stats(const cmc_server* server, cmc_server_stats* out) {
+    if (!server || !out) return CMC_EINVAL;
+    *out = reinterpret_cast<const Server*>(server)->stats;
+    return CMC_OK;
+}
+
 uint32_t cmc_server_pending(const cmc_server* server) {
     if (!server) return 0;
     const Server* s = reinterpret_cast<const Server*>(server);
@@ -623,8 +809,12 @@ const char* cmc_server_error(const cmc_server* server) {
 }
 
 int cmc_server_destroy(cmc_server* server) {
-    delete reinterpret_cast<Server*>(server);
-    return CMC_OK;
+    if (!server) return CMC_OK;
+    Server* s = reinterpret_cast<Server*>(server);
+    const int rc = s->drain();  // commit what the device finished
+    if (rc) s->ctx->err = s->err;
+    delete s;
+    return rc;
 }
 
 }  // extern "C"

@@ -19,6 +19,8 @@ ENGINE_VARIANTS = [
     {"walkers": 2, "warps_per_group": 7, "isolate_walkers": 0},
     {"isolate_walkers": 1, "warps_per_group": 6, "walkers": 3},
     {"isolate_walkers": 1, "warps_per_group": 1, "global_slots": 1},
+    {"method": 2},                             # round cache in global memory (h <= 16)
+    {"method": 2, "isolate_walkers": 1, "global_slots": 1, "warps_per_group": 4},
 ]
 
 
@@ -81,7 +83,7 @@ def reference_cases(golden):
     return [r["name"] for r in golden["reference_runs"]]
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 6, 7, 9, 10])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 6, 7, 9, 10, 11, 12])
 def test_reference_runs(ctx, cmc, golden, variant):
     apply(ctx, ENGINE_VARIANTS[variant])
     for r in golden["reference_runs"]:
@@ -110,7 +112,7 @@ def random_shapes(n, seed):
 @pytest.mark.parametrize("shape", random_shapes(24, 7))
 def test_vs_oracle_random_shapes(ctx, cmc, oracle, shape):
     mode, im, pnum, ell, k, buckets, kick, seed, batch = shape
-    apply(ctx, ENGINE_VARIANTS[[0, 6, 7, 9, 10][seed % 5]])
+    apply(ctx, ENGINE_VARIANTS[[0, 6, 7, 9, 10, 11, 12][seed % 7]])
     p = cmc.parameters(mode, pnum, ell, k, buckets, kick, im)
     op = oracle.params(mode, pnum, ell, k, buckets, kick, im)
     count = 512 if pnum <= 100 else 96
@@ -137,6 +139,23 @@ def test_wide_domain(ctx, cmc, oracle):
     want = oracle.batch(op, 5, 1, 0, 256)
     assert ctx.launch(p, cmc.batch_key(5, 1), 0, 256) == want
     assert "wide-domain" in ctx.last_plan
+
+
+@pytest.mark.parametrize("method", [0, 2])
+def test_global_round_cache_h13_to_16(ctx, cmc, oracle, method):
+    # half widths 13..16: direct passes and the L2-resident round cache agree
+    # with the oracle trial for trial
+    for mode, pnum, ell, k, buckets, kick, seed in [
+            ("bgh25", 3000, 24, 3, 3900, 100, 21),      # h = 13
+            ("drrt18", 1500, 24, 4, 1900, 60, 22),      # h = 14
+            ("bgh25", 600, 28, 3, 700, 200, 23),        # h = 15
+            ("bgh25", 200, 28, 4, 260, 100, 24)]:       # h = 16
+        p = cmc.parameters(mode, pnum, ell, k, buckets, kick, "affine")
+        op = oracle.params(mode, pnum, ell, k, buckets, kick, "affine")
+        ctx.set_option("method", method)
+        want = oracle.batch(op, seed, 1, 50, 64)
+        assert ctx.launch(p, cmc.batch_key(seed, 1), 50, 64) == want, (p.half_bits, ctx.last_plan)
+        assert ("cache=global" in ctx.last_plan) == (method == 2)
 
 
 def test_launch_device_matches_host(ctx, cmc):

@@ -44,6 +44,11 @@ def test_served_equals_alone(ctx, cmc, tmp_path):
         steps += 1
         assert steps < 10000
     assert finished == set(ids)
+    st = srv.stats()
+    total = sum(-(-b // (1 << min(bt, max(1, (b - 1).bit_length())))) << min(bt, max(1, (b - 1).bit_length()))
+                for _, _, b in jobs)
+    assert st["trials"] == total and st["iterations"] >= 1
+    assert 0 < st["busy_ms"] <= st["engine_ms"] + 1e-3 and st["busy_ms"] <= st["span_ms"] + 1e-3
     for i, (p, seed, budget) in enumerate(jobs):
         per = 1 << min(bt, max(1, (budget - 1).bit_length()))
         got = cmc.read_journal(tmp_path / f"job{i}" / "worker_0.bin")
