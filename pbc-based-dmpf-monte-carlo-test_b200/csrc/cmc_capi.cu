@@ -254,96 +254,140 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     return CMC_OK;
 }
 
-// Queue one engine launch over `jobs` (already on the device in d_jobs) and
-// the compaction of its failure bitmap.
+// Queue the engine launches over `jobs` (already on the device in d_jobs) --
+// one per plan class, class c covering the job-table range
+// [bounds[c], bounds[c + 1]) and so a contiguous range of global trial
+// indices -- and the compaction of the shared failure bitmap.
 int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint32_t value_base,
              uint32_t* d_out, uint32_t* d_count, uint64_t out_cap_now,
-             unsigned long long* job_failed, unsigned long long* job_done) {
-    Plan pl;
-    int rc = plan(jobs, pl);
-    if (rc) return rc;
-    const size_t words = (total + 31) / 32;
-    if ((rc = grow(d_bits, bits_cap, words, "failure bitmap"))) return rc;
-    // one global pool: walk slots, then the groups' round caches
-    const size_t cache_off = size_t((pl.gslot_bytes + 255) / 256 * 256);
-    if (pl.gslot_bytes || pl.gcache_bytes)
-        if ((rc = grow(d_slots, slots_cap, cache_off + pl.gcache_bytes, "slot and cache pool"))) return rc;
-    if (pl.walker_ctas) {
-        if ((rc = grow(d_ghdr, ghdr_cap, pl.ns, "slot headers"))) return rc;
-        if ((rc = cuda(cudaMemsetAsync(d_ghdr, 0, size_t(pl.ns) * sizeof(GSlotHeader), st), "memset slots")))
-            return rc;
+             unsigned long long* job_failed, unsigned long long* job_done,
+             const std::vector<uint32_t>* bounds_in) {
+    std::vector<uint32_t> bounds = bounds_in ? *bounds_in : std::vector<uint32_t>{0, uint32_t(jobs.size())};
+    const uint32_t nclass = uint32_t(bounds.size()) - 1;
+    if (nclass < 1 || nclass > kMaxClasses) return fail(CMC_EINVAL, "bad plan classes");
+    std::vector<Plan> plans(nclass);
+    uint64_t pool = 0;
+    uint32_t heaviest = 0;
+    uint64_t heaviest_trials = 0;
+    std::string text;
+    for (uint32_t c = 0; c < nclass; ++c) {
+        std::vector<Job> part(jobs.begin() + bounds[c], jobs.begin() + bounds[c + 1]);
+        int rc = plan(part, plans[c]);
+        if (rc) return rc;
+        const Plan& pl = plans[c];
+        pool = std::max<uint64_t>(pool, (pl.gslot_bytes + 255) / 256 * 256 + pl.gcache_bytes);
+        uint64_t trials = 0;
+        for (const Job& j : part) trials += j.count;
+        if (trials > heaviest_trials) {
+            heaviest_trials = trials;
+            heaviest = c;
+        }
+        text += (c ? " | " : "") + plan_text;
     }
-    if ((rc = cuda(cudaMemsetAsync(d_ctrl, 0, sizeof(Ctrl), st), "memset ctrl"))) return rc;
+    plan_text = text;
+    const size_t words = (total + 31) / 32;
+    int rc = grow(d_bits, bits_cap, words, "failure bitmap");
+    if (rc) return rc;
+    // one global pool per launch, reused by the classes in stream order:
+    // walk slots, then the groups' round caches
+    if (pool && (rc = grow(d_slots, slots_cap, size_t(pool), "slot and cache pool"))) return rc;
+    if ((rc = cuda(cudaMemsetAsync(d_ctrl, 0, nclass * sizeof(Ctrl), st), "memset ctrl"))) return rc;
     if ((rc = cuda(cudaMemsetAsync(d_bits, 0, words * 4, st), "memset bitmap"))) return rc;
-    EngineArgs a{};
-    a.jobs = d_jobs;
-    a.njobs = uint32_t(jobs.size());
-    a.total = total;
-    a.ctrl = d_ctrl;
-    a.fail_bits = d_bits;
-    a.job_failed = job_failed;
-    a.job_done = job_done;
-    a.gslots = pl.slots_smem ? nullptr : d_slots;
-    a.gcache = pl.gcache_bytes ? reinterpret_cast<uint16_t*>(d_slots + cache_off) : nullptr;
-    a.gcache_stride = pl.gcache_stride;
-    a.ghdr = pl.walker_ctas ? d_ghdr : nullptr;
-    a.split = pl.walker_ctas ? 1 : 0;
-    a.producer_ctas = pl.ctas - pl.walker_ctas;
-    a.total_groups = a.producer_ctas * pl.ng;
-    a.t0 = d_t0;
-    a.slot_stride = pl.slot_stride;
-    a.bins_bytes = pl.bins_bytes;
-    a.ng = pl.ng;
-    a.wg = pl.wg;
-    a.ns = pl.ns;
-    a.nw = pl.nw;
-    a.isolate_walkers = pl.isolate;
-    a.r256 = 256u;
-    a.group_bytes = pl.group_bytes;
-    a.group_off = pl.group_off;
-    a.slots_off = pl.slots_off;
-    a.spin_limit = spin_limit;
-    const void* fn =
-        pl.walker_ctas
-            ? (pl.variant == 0   ? (const void*)cmc_engine_split<uint16_t, uint16_t, false>
-               : pl.variant == 1 ? (const void*)cmc_engine_split<uint32_t, uint32_t, false>
-                                 : (const void*)cmc_engine_split<uint32_t, uint32_t, true>)
-            : (pl.variant == 0   ? (const void*)cmc_engine<uint16_t, uint16_t, false>
-               : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
-                                 : (const void*)cmc_engine<uint32_t, uint32_t, true>);
-    if ((rc = cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(pl.smem_bytes)),
-                   "cudaFuncSetAttribute")))
-        return rc;
-    void* args[] = {&a};
     if ((rc = cuda(cudaEventRecord(ev_start, st), "event"))) return rc;
-    // The split engine's producer and walker CTAs hand trials to each other, so
-    // they must all be resident at once: a cooperative launch guarantees it.
-    if ((rc = cuda(pl.walker_ctas ? cudaLaunchCooperativeKernel(fn, dim3(pl.ctas), dim3(pl.threads),
-                                                                 args, pl.smem_bytes, st)
-                                  : cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args,
-                                                     pl.smem_bytes, st),
-                   "engine launch")))
-        return rc;
+    kernels = 0;
+    for (uint32_t c = 0; c < nclass; ++c) {
+        const Plan& pl = plans[c];
+        if (pl.walker_ctas) {
+            if ((rc = grow(d_ghdr, ghdr_cap, pl.ns, "slot headers"))) return rc;
+            if ((rc = cuda(cudaMemsetAsync(d_ghdr, 0, size_t(pl.ns) * sizeof(GSlotHeader), st), "memset slots")))
+                return rc;
+        }
+        const size_t cache_off = size_t((pl.gslot_bytes + 255) / 256 * 256);
+        EngineArgs a{};
+        a.jobs = d_jobs;
+        a.njobs = uint32_t(jobs.size());
+        a.gidx_begin = jobs[bounds[c]].trial_base;
+        a.total = bounds[c + 1] < jobs.size() ? jobs[bounds[c + 1]].trial_base : total;
+        a.ctrl = d_ctrl + c;
+        a.fail_bits = d_bits;
+        a.job_failed = job_failed;
+        a.job_done = job_done;
+        a.gslots = pl.slots_smem ? nullptr : d_slots;
+        a.gcache = pl.gcache_bytes ? reinterpret_cast<uint16_t*>(d_slots + cache_off) : nullptr;
+        a.gcache_stride = pl.gcache_stride;
+        a.ghdr = pl.walker_ctas ? d_ghdr : nullptr;
+        a.split = pl.walker_ctas ? 1 : 0;
+        a.producer_ctas = pl.ctas - pl.walker_ctas;
+        a.total_groups = a.producer_ctas * pl.ng;
+        a.t0 = d_t0;
+        a.slot_stride = pl.slot_stride;
+        a.bins_bytes = pl.bins_bytes;
+        a.ng = pl.ng;
+        a.wg = pl.wg;
+        a.ns = pl.ns;
+        a.nw = pl.nw;
+        a.isolate_walkers = pl.isolate;
+        a.r256 = 256u;
+        a.group_bytes = pl.group_bytes;
+        a.group_off = pl.group_off;
+        a.slots_off = pl.slots_off;
+        a.spin_limit = spin_limit;
+        const void* fn =
+            pl.walker_ctas
+                ? (pl.variant == 0   ? (const void*)cmc_engine_split<uint16_t, uint16_t, false>
+                   : pl.variant == 1 ? (const void*)cmc_engine_split<uint32_t, uint32_t, false>
+                                     : (const void*)cmc_engine_split<uint32_t, uint32_t, true>)
+                : (pl.variant == 0   ? (const void*)cmc_engine<uint16_t, uint16_t, false>
+                   : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
+                                     : (const void*)cmc_engine<uint32_t, uint32_t, true>);
+        if ((rc = cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(pl.smem_bytes)),
+                       "cudaFuncSetAttribute")))
+            return rc;
+        void* args[] = {&a};
+        // The split engine's producer and walker CTAs hand trials to each other, so
+        // they must all be resident at once: a cooperative launch guarantees it.
+        if ((rc = cuda(pl.walker_ctas ? cudaLaunchCooperativeKernel(fn, dim3(pl.ctas), dim3(pl.threads),
+                                                                     args, pl.smem_bytes, st)
+                                      : cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args,
+                                                         pl.smem_bytes, st),
+                       "engine launch")))
+            return rc;
+        ++kernels;
+    }
     if ((rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
-    kernels = 1;
     if (d_out) {
         cmc_compact_failures<<<1, 1024, 0, st>>>(d_bits, total, value_base, d_out, d_count, out_cap_now,
                                                  nullptr);
         if ((rc = cuda(cudaGetLastError(), "compaction launch"))) return rc;
-        kernels = 2;
+        ++kernels;
     }
-    last_plan = pl;
+    last_plan = plans[heaviest];
+    ctrl_count = nclass;
     return CMC_OK;
 }
 
 int Ctx::check_ctrl() {
-    Ctrl c{};
-    int rc = cuda(cudaMemcpy(&c, d_ctrl, sizeof c, cudaMemcpyDeviceToHost), "read ctrl");
+    Ctrl c[kMaxClasses]{};
+    const uint32_t n = std::max<uint32_t>(1, ctrl_count);
+    int rc = cuda(cudaMemcpy(c, d_ctrl, n * sizeof(Ctrl), cudaMemcpyDeviceToHost), "read ctrl");
     if (rc) return rc;
-    last_ctrl = c;
-    if (c.error)
-        return fail(-int(c.error), "device wait gave up (site %u): results discarded", c.where);
+    Ctrl sum{};
+    for (uint32_t i = 0; i < n; ++i) {
+        if (c[i].error && !sum.error) {
+            sum.error = c[i].error;
+            sum.where = c[i].where;
+        }
+        sum.next += c[i].next;
+        sum.walks += c[i].walks;
+        sum.probes += c[i].probes;
+        sum.slot_wait_cycles += c[i].slot_wait_cycles;
+        sum.walker_idle_cycles += c[i].walker_idle_cycles;
+        sum.walker_cycles += c[i].walker_cycles;
+    }
+    last_ctrl = sum;
+    if (sum.error)
+        return fail(-int(sum.error), "device wait gave up (site %u): results discarded", sum.where);
     return CMC_OK;
 }
 
@@ -371,7 +415,7 @@ int Ctx::init(int dev) {
     if ((rc = cuda(cudaMemcpy(d_t0 + 256, fips, sizeof fips, cudaMemcpyHostToDevice), "upload KAT key")))
         return rc;
     size_t c1 = 0;
-    if ((rc = grow(d_ctrl, c1, 1, "ctrl"))) return rc;
+    if ((rc = grow(d_ctrl, c1, kMaxClasses, "ctrl"))) return rc;
     const uint32_t kat_smem = kEngineTableBytes;
     if ((rc = cuda(cudaFuncSetAttribute((const void*)cmc_selftest,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kat_smem),
@@ -489,7 +533,7 @@ std::string Ctx::mix_key(const cmc_job* in, uint32_t n) const {
 }
 
 int Ctx::prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::vector<Job>& out,
-                      std::vector<uint32_t>& order, uint64_t& total) {
+                      std::vector<uint32_t>& order, uint64_t& total, std::vector<uint32_t>& bounds) {
     if (!in || n == 0) return fail(CMC_EINVAL, "no jobs");
     std::vector<Job> tmp(n);
     for (uint32_t i = 0; i < n; ++i) {
@@ -503,10 +547,46 @@ int Ctx::prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::v
         batch_key(in[i].seed, in[i].batch, tmp[i].batch_rk);
         tmp[i].user = i;
     }
+    // Plan classes: parameter sets whose own plans agree (slot placement,
+    // warps per group, groups, walkers, entry width, cache kind) run in one
+    // launch under that plan, so a small table never runs under a plan made
+    // for a large one.  Classes run heaviest first; within a class, heaviest
+    // trials first, so a launch ends on short ones.  Past kMaxClasses
+    // signatures the lightest classes share the last launch.
+    std::vector<uint32_t> cls(n, 0);
+    if (force_walker_ctas <= 0) {
+        std::map<std::string, uint32_t> ids;
+        std::vector<double> weight;
+        std::vector<uint32_t> sig(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            Plan solo;
+            int rc = plan(std::vector<Job>{tmp[i]}, solo);
+            if (rc) return rc;
+            const char cache = tmp[i].method == kMethodCache ? 's' : tmp[i].method == kMethodGCache ? 'g' : 'd';
+            char key[96];
+            snprintf(key, sizeof key, "%d/%u/%u/%u/%u/%d/%c", solo.slots_smem ? 1 : 0, solo.wg, solo.ng,
+                     solo.nw, solo.isolate, solo.variant, cache);
+            auto it = ids.emplace(key, uint32_t(ids.size())).first;
+            sig[i] = it->second;
+            if (weight.size() <= sig[i]) weight.resize(sig[i] + 1, 0.0);
+            weight[sig[i]] += job_cost(tmp[i]) * tmp[i].count;
+        }
+        std::vector<uint32_t> rank(weight.size());
+        for (uint32_t c = 0; c < rank.size(); ++c) rank[c] = c;
+        std::stable_sort(rank.begin(), rank.end(), [&](uint32_t a, uint32_t b) { return weight[a] > weight[b]; });
+        std::vector<uint32_t> pos(rank.size());
+        for (uint32_t r = 0; r < rank.size(); ++r) pos[rank[r]] = std::min<uint32_t>(r, kMaxClasses - 1);
+        for (uint32_t i = 0; i < n; ++i) cls[i] = pos[sig[i]];
+    }
     order.resize(n);
     for (uint32_t i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t a, uint32_t b) { return job_cost(tmp[a]) > job_cost(tmp[b]); });
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        return cls[a] != cls[b] ? cls[a] < cls[b] : job_cost(tmp[a]) > job_cost(tmp[b]);
+    });
+    bounds.assign(1, 0);
+    for (uint32_t i = 1; i < n; ++i)
+        if (cls[order[i]] != cls[order[i - 1]]) bounds.push_back(i);
+    bounds.push_back(n);
     out.resize(n);
     total = 0;
     for (uint32_t i = 0; i < n; ++i) {
@@ -551,9 +631,9 @@ int Ctx::run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t*
     const auto it = tuned.find(mix_key(in, n));
     ScopedPlan scoped(*this, it == tuned.end() ? nullptr : &it->second);
     std::vector<Job> jobs;
-    std::vector<uint32_t> order;
+    std::vector<uint32_t> order, bounds;
     uint64_t total = 0;
-    if ((rc = prepare_jobs(in, n, 0, jobs, order, total))) return rc;
+    if ((rc = prepare_jobs(in, n, 0, jobs, order, total, bounds))) return rc;
     cudaStream_t st = user_stream ? user_stream : stream;
     if ((rc = upload_jobs(jobs, st))) return rc;
     if ((rc = grow(d_job_failed, job_failed_cap, n, "job counters"))) return rc;
@@ -561,7 +641,8 @@ int Ctx::run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t*
         return rc;
     const uint64_t dev_cap = out_offsets ? std::min<uint64_t>(cap, total) : 0;
     if ((rc = grow(d_out, out_cap, size_t(dev_cap) + 1, "failure list"))) return rc;
-    if ((rc = run(jobs, total, st, 0, d_out, d_out + dev_cap, dev_cap, d_job_failed, nullptr))) return rc;
+    if ((rc = run(jobs, total, st, 0, d_out, d_out + dev_cap, dev_cap, d_job_failed, nullptr, &bounds)))
+        return rc;
     std::vector<unsigned long long> failed(n);
     uint32_t nf = 0;
     if ((rc = cuda(cudaMemcpyAsync(failed.data(), d_job_failed, n * sizeof(unsigned long long),
@@ -606,13 +687,13 @@ int Ctx::autotune(const cmc_job* in, uint32_t n, uint32_t sample_div) {
     int rc = cuda(cudaSetDevice(device), "cudaSetDevice");
     if (rc) return rc;
     std::vector<Job> jobs;
-    std::vector<uint32_t> order;
+    std::vector<uint32_t> order, bounds;
     uint64_t total = 0;
-    if ((rc = prepare_jobs(in, n, sample_div ? sample_div : 64, jobs, order, total))) return rc;
+    if ((rc = prepare_jobs(in, n, sample_div ? sample_div : 64, jobs, order, total, bounds))) return rc;
     cudaStream_t st = user_stream ? user_stream : stream;
     bool any_cached = false;  // does the automatic choice use a round cache anywhere?
     for (const Job& j : jobs) any_cached = any_cached || j.method != kMethodDirect;
-    std::vector<TunedPlan> cands;
+    std::vector<TunedPlan> cands{TunedPlan{0, -1, -1}};  // each class under its automatic plan
     for (int iso : {0, 1})
         for (uint32_t wg : {1u, 2u, 4u, 6u})
             for (int method : {-1, 0}) {
@@ -633,7 +714,7 @@ int Ctx::autotune(const cmc_job* in, uint32_t n, uint32_t sample_div) {
             js[i].method = tmp.method;
         }
         if ((rc = upload_jobs(js, st))) return rc;
-        rc = run(js, total, st, 0, nullptr, nullptr, 0, d_job_failed, nullptr);
+        rc = run(js, total, st, 0, nullptr, nullptr, 0, d_job_failed, nullptr, &bounds);
         if (rc == CMC_EINVAL) continue;  // plan does not fit: skip the candidate
         if (rc) return rc;
         float ms = 0;

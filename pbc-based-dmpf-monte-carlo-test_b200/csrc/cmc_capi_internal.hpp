@@ -12,6 +12,8 @@
 
 namespace cmc {
 
+constexpr uint32_t kMaxClasses = 16;  // plan classes (engine launches) per batched call
+
 struct Plan {
     uint32_t ng = 0, wg = 0, ns = 0, nw = 1;
     uint32_t walker_ctas = 0;  // > 0: split engine with this many walker CTAs
@@ -44,7 +46,8 @@ struct Ctx {
     cudaStream_t user_stream = nullptr;  // cmc_set_stream override
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     uint32_t* d_t0 = nullptr;  // T0 table, FIPS KAT schedule, self-test output
-    Ctrl* d_ctrl = nullptr;
+    Ctrl* d_ctrl = nullptr;      // one control block per plan class of a launch
+    uint32_t ctrl_count = 1;     // control blocks the last run used
     Job* d_jobs = nullptr;
     size_t jobs_cap = 0;
     uint32_t* d_bits = nullptr;
@@ -84,14 +87,14 @@ struct Ctx {
     int upload_jobs(const std::vector<Job>& jobs, cudaStream_t st);
     int run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint32_t value_base,
             uint32_t* d_out, uint32_t* d_count, uint64_t out_cap, unsigned long long* job_failed,
-            unsigned long long* job_done);
+            unsigned long long* job_done, const std::vector<uint32_t>* class_bounds = nullptr);
     int check_ctrl();
     int launch_host(const cmc_params& p, const uint32_t key[44], uint32_t first, uint32_t count,
                     uint32_t* out, uint32_t* nfailed);
     int launch_device(const cmc_params& p, const uint32_t* d_key, uint32_t first, uint32_t count,
                       uint32_t* d_offsets, uint32_t* d_nfailed, cudaStream_t st);
     int prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::vector<Job>& out,
-                     std::vector<uint32_t>& order, uint64_t& total);
+                     std::vector<uint32_t>& order, uint64_t& total, std::vector<uint32_t>& bounds);
     std::string mix_key(const cmc_job* in, uint32_t n) const;
     int run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t* out_offsets,
                  uint32_t* out_jobs, uint64_t cap, uint64_t* out_total);

@@ -291,7 +291,7 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
 
     for (;;) {
         if (gt == 0) {
-            const unsigned long long gi = atomicAdd(&a.ctrl->next, 1ULL);
+            const unsigned long long gi = a.gidx_begin + atomicAdd(&a.ctrl->next, 1ULL);
             gh->gidx = gi;
             gh->abort = 0;
             if (gi < total) {

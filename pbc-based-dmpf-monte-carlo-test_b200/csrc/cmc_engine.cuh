@@ -19,8 +19,8 @@ constexpr uint32_t kEngineTableBytes = 65536;  // replicated T-table at shared o
 constexpr uint32_t kMaxGroups = 14; // named barriers 1..14
 
 // One experiment configuration applied to a contiguous run of trials of one
-// batch.  A launch processes trials [0, total) of the concatenation of its
-// jobs; job j owns global indices [trial_base, trial_base + count).
+// batch.  The job table concatenates its jobs' trials: job j owns global
+// indices [trial_base, trial_base + count); a launch runs a contiguous range.
 struct Job {
     uint32_t batch_rk[44];  // batch key schedule (plain words)
     uint32_t pnum, k, buckets, kick;
@@ -56,7 +56,8 @@ struct __align__(64) GSlotHeader {
 struct EngineArgs {
     const Job* jobs;
     uint32_t njobs;
-    uint64_t total;
+    uint64_t total;                     // the launch runs global trials [gidx_begin, total)
+    uint64_t gidx_begin;
     Ctrl* ctrl;
     uint32_t* fail_bits;                // bit g = global trial g failed
     unsigned long long* job_failed;     // per job (optional)

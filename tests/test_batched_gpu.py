@@ -49,3 +49,17 @@ def test_capacity_limits_offsets_not_counts(ctx, cmc):
     assert failed[0] > 5 and len(per_job[0]) == 5
     full = ctx.launch(jobs[0][0], cmc.batch_key(3, 0), 0, 2000)
     assert failed[0] == len(full)
+
+
+def test_plan_classes(ctx, cmc):
+    # long-walk sets (global walk slots) and short ones (shared-memory slots)
+    # run as separate launches of one call, each under its own plan
+    jobs = [(cmc.parameters("bgh25", 8000, 24, 3, 11200, 500, "affine"), 5, 0, 0, 96),
+            (cmc.parameters("bgh25", 64, 16, 3, 80, 50, "affine"), 11, 1, 10, 3000),
+            (cmc.parameters("drrt18", 3000, 24, 2, 3600, 100, "affine"), 6, 2, 0, 64),
+            (cmc.parameters("bgh25", 300, 20, 4, 340, 100, "sequential"), 7, 0, 5, 700)]
+    failed, per_job = ctx.run_jobs(jobs)
+    assert " | " in ctx.last_plan and ctx.last_kernel_count >= 3
+    for i, (p, s, b, first, count) in enumerate(jobs):
+        assert per_job[i] == ctx.launch(p, cmc.batch_key(s, b), first, count), i
+        assert failed[i] == len(per_job[i])
