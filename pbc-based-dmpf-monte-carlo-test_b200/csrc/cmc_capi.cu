@@ -31,7 +31,6 @@ namespace {
 
 thread_local std::string g_thread_error;
 
-constexpr uint32_t kGroupHeaderBytes = 512;
 
 uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 

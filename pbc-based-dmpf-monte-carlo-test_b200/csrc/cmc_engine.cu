@@ -38,8 +38,11 @@ struct GroupHeader {
     uint32_t rk[44];
     uint32_t r1[8][8];  // Round1 {c0, c1, c2, c3, w3hi} per Feistel round (padded)
     unsigned long long walk, rnd, shift, step;
-    uint32_t slot, cand_next, abort, pad;
+    uint32_t slot, cand_next, abort, live;
+    unsigned long long entry;  // resident launch: ring entry of the last trial
+    Job jd;                    // this trial's job descriptor, read at L2
 };
+static_assert(sizeof(GroupHeader) <= kGroupHeaderBytes, "the planner reserves kGroupHeaderBytes");
 
 struct SlotHeader {
     unsigned long long gidx, walk, rnd;
@@ -74,6 +77,18 @@ __device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
 __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_sys(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -289,21 +304,78 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
     uint32_t cursor = 0;
     const unsigned long long total = a.total_dev ? *a.total_dev : a.total;
 
+    if (gt == 0) gh->entry = a.entry_begin;
     for (;;) {
         if (gt == 0) {
             const unsigned long long gi = a.gidx_begin + atomicAdd(&a.ctrl->next, 1ULL);
             gh->gidx = gi;
             gh->abort = 0;
-            if (gi < total) {
+            uint32_t live = gi < total;
+            if (a.rq) {
+                // Resident: wait until trial gi is published or the host
+                // closes the launch.  Claims rise, so a group that leaves
+                // holds an index past the final `avail`: every published
+                // trial is taken by some group.
+                live = 0;
+                uint32_t spins = 0;
+                for (;;) {
+                    const uint32_t stop = ld_acquire_sys(&a.rq->stop);
+                    if (gi < ld_acquire_sys(&a.rq->avail)) {
+                        live = 1;
+                        break;
+                    }
+                    if (stop) break;
+                    __nanosleep(1024);
+                    if (++spins > a.spin_limit) {
+                        atomicExch(&a.ctrl->error, kErrTimeout);
+                        atomicExch(&a.ctrl->where, 4u);
+                        break;
+                    }
+                }
+                if (live) {
+                    // the entry holding gi: entries are published in order
+                    unsigned long long e = gh->entry;
+                    uint32_t steps = 0;
+                    for (;;) {
+                        const Job* je = &a.jobs[e & a.ring_mask];
+                        const unsigned long long base = __ldcg(&je->trial_base);
+                        if (gi >= base && gi - base < __ldcg(&je->count)) {
+                            gh->offset = __ldcg(&je->first) + (uint32_t)(gi - base);
+                            break;
+                        }
+                        ++e;
+                        if (++steps > a.ring_mask + 1) {  // inconsistent ring: never spin on it
+                            atomicExch(&a.ctrl->error, kErrRange);
+                            atomicExch(&a.ctrl->where, 5u);
+                            live = 0;
+                            break;
+                        }
+                    }
+                    gh->entry = e;
+                    gh->job = (uint32_t)(e & a.ring_mask);
+                    // this trial's failure bit starts clear (the ring reuses bits)
+                    if (live)
+                        atomicAnd(&a.fail_bits[(gi & a.bits_mask) >> 5], ~(1u << (gi & 31)));
+                }
+            } else if (live) {
                 const uint32_t j = find_job(a.jobs, a.njobs, gi);
                 gh->job = j;
                 gh->offset = a.jobs[j].first + (uint32_t)(gi - a.jobs[j].trial_base);
             }
+            gh->live = live;
         }
         group_sync(g, gthreads);
+        if (!gh->live) break;
         const unsigned long long gi = gh->gidx;
-        if (gi >= total) break;
-        const Job& J = a.jobs[gh->job];
+        {
+            // this trial's job descriptor, read at L2: a resident ring entry
+            // may have been rewritten since an earlier trial read it
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(&a.jobs[gh->job]);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&gh->jd);
+            for (uint32_t i = gt; i < sizeof(Job) / 4; i += gthreads) dst[i] = __ldcg(src + i);
+        }
+        group_sync(g, gthreads);
+        const Job& J = gh->jd;
 
         // Per-trial PRP key and walk seed (cuckoo_bench.cu:226-238).
         if (gt == 0) {
@@ -492,11 +564,13 @@ struct Walk {
         mem.bind(a, slot);
         walk = h.walk;
         rnd = h.rnd;
-        k = J.k;
-        t = J.pnum;
-        kick = J.kick;
-        nbins = J.buckets;
-        bgh = J.mode == 1;
+        // at L2: a resident ring entry may have been rewritten since this SM
+        // last read it
+        k = __ldcg(&J.k);
+        t = __ldcg(&J.pnum);
+        kick = __ldcg(&J.kick);
+        nbins = __ldcg(&J.buckets);
+        bgh = __ldcg(&J.mode) == 1;
         // rnd / k == umulhi(rnd, magic) >> magic_shift for k in {2, 3, 4}
         magic = k == 3 ? 0xAAAAAAAAAAAAAAABULL : (k == 2 ? 0x8000000000000000ULL : 0x4000000000000000ULL);
         magic_shift = k == 3 ? 1 : 0;
@@ -655,12 +729,17 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
                 atomicExch(&a.ctrl->error, kErrRange);
                 atomicExch(&a.ctrl->where, 3u);
             }
-            const uint32_t cidx = a.count_by_user ? a.jobs[job].user : job;
+            const uint32_t cidx = a.count_by_user ? __ldcg(&a.jobs[job].user) : job;
             if (w.failed) {
-                atomicOr(&a.fail_bits[gidx >> 5], 1u << (gidx & 31));
+                const unsigned long long bit = a.bits_mask ? (gidx & a.bits_mask) : gidx;
+                atomicOr(&a.fail_bits[bit >> 5], 1u << (bit & 31));
                 if (a.job_failed) atomicAdd(&a.job_failed[cidx], 1ULL);
             }
             if (a.job_done) atomicAdd(&a.job_done[cidx], 1ULL);
+            if (a.entry_done) {
+                __threadfence();  // the failure bit is visible before the count
+                atomicAdd(&a.entry_done[job], 1u);
+            }
             ++walks;
             busy = false;
             __threadfence_block();
@@ -737,12 +816,17 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
                 atomicExch(&a.ctrl->error, kErrRange);
                 atomicExch(&a.ctrl->where, 3u);
             }
-            const uint32_t cidx = a.count_by_user ? a.jobs[job].user : job;
+            const uint32_t cidx = a.count_by_user ? __ldcg(&a.jobs[job].user) : job;
             if (w.failed) {
-                atomicOr(&a.fail_bits[gidx >> 5], 1u << (gidx & 31));
+                const unsigned long long bit = a.bits_mask ? (gidx & a.bits_mask) : gidx;
+                atomicOr(&a.fail_bits[bit >> 5], 1u << (bit & 31));
                 if (a.job_failed) atomicAdd(&a.job_failed[cidx], 1ULL);
             }
             if (a.job_done) atomicAdd(&a.job_done[cidx], 1ULL);
+            if (a.entry_done) {
+                __threadfence();  // the failure bit is visible before the count
+                atomicAdd(&a.entry_done[job], 1u);
+            }
             ++walks;
             busy = false;
             __threadfence();

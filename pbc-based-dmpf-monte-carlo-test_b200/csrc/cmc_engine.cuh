@@ -17,6 +17,7 @@ constexpr uint32_t kMaxSlots = 128;  // one walker lane per slot, up to 4 walker
 constexpr uint32_t kCtaSharedBytes = 4864;  // slot states and headers after the T-table
 constexpr uint32_t kEngineTableBytes = 65536;  // replicated T-table at shared offset 0
 constexpr uint32_t kMaxGroups = 14; // named barriers 1..14
+constexpr uint32_t kGroupHeaderBytes = 1024;  // per-group shared header (the trial's job copy)
 
 // One experiment configuration applied to a contiguous run of trials of one
 // batch.  The job table concatenates its jobs' trials: job j owns global
@@ -44,6 +45,14 @@ struct Ctrl {
     unsigned long long walker_cycles;      // walker warps' lifetime
     unsigned int slot_cursor;              // split engine: next slot to try
     unsigned int groups_done;              // split engine: producer groups finished
+};
+
+// Resident launches: the host publishes work while the kernel runs.  Lives
+// in mapped pinned host memory; the host writes `avail` before `stop`.
+struct ResidentQueue {
+    unsigned long long avail;  // trials with global index < avail are published
+    unsigned int stop;         // 1: no more work in this launch
+    unsigned int pad;
 };
 
 // Split engine: header of one global slot (one walker thread per slot).
@@ -87,6 +96,16 @@ struct EngineArgs {
     // [(cta * ng + g) * gcache_stride, +8 << h)
     uint16_t* gcache;
     uint32_t gcache_stride;
+    // resident launch (rq != nullptr): `jobs` is a ring of ring_mask + 1
+    // entries that the host fills ahead of `avail`; trial g belongs to the
+    // first entry, scanning forward from entry_begin, whose range holds it;
+    // the failure bitmap is a ring of bits_mask + 1 bits (bits_mask 0: no
+    // ring); entry_done[e] counts the finished walks of ring entry e
+    const ResidentQueue* rq;
+    uint32_t ring_mask;
+    unsigned long long entry_begin;
+    unsigned long long bits_mask;
+    unsigned int* entry_done;
 };
 
 // Serving: device-resident state of one admitted job.  `next` is the job's
