@@ -351,6 +351,7 @@ def run_serve_workload(args):
     srv = cmc.Server(ctx, max_jobs=4096, mem_budget=8 << 30, batch_bits=20,
                      max_iteration_trials=1 << 23)
     srv.policy(args.serve_fifo_share)
+    srv.set_option("resident", args.serve_resident)
     t0 = time.perf_counter()
     submitted, done_at, ids = 0, {}, {}
     while len(done_at) < len(jobs):
@@ -401,7 +402,7 @@ def run_serve_workload(args):
                   "trials_per_s": total_trials / plain_span, "makespan_s": plain_span},
         "identical_failure_counts": served_failed == plain_failed,
         "total_trials": total_trials, "step_blocks": args.serve_step_blocks,
-        "fifo_share": args.serve_fifo_share,
+        "fifo_share": args.serve_fifo_share, "resident": args.serve_resident,
         "timing": "host wall clock from each job's arrival to its completion",
     }
     print(json.dumps(line), flush=True)
@@ -425,6 +426,8 @@ def main():
     ap.add_argument("--serve-log2-budget", default="10,16")
     ap.add_argument("--serve-step-blocks", type=int, default=400_000_000)
     ap.add_argument("--serve-fifo-share", type=float, default=0.95)
+    ap.add_argument("--serve-resident", type=int, default=1, choices=[0, 1],
+                    help="1: one resident engine launch per busy period; 0: one launch per iteration")
     ap.add_argument("--sweep-trials", type=int, default=1 << 16,
                     help="trials per parameter set for --workload sweep")
     args = ap.parse_args()

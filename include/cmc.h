@@ -156,6 +156,15 @@ int cmc_server_status(cmc_server* server, uint32_t job_id, uint64_t* out_trials_
  * measured on a 400-job stream, 0.95 keeps p99 at or below plain launches at
  * 60 and 200 jobs/s while halving p50; 0.5 cuts p50 by 5x but raises p99. */
 int cmc_server_policy(cmc_server* server, double fifo_share);
+/* Server options: "fifo_share" (as cmc_server_policy) and "resident" (0 or
+ * 1, default 1).  Resident serving keeps one engine launch on the device
+ * while jobs are pending: each step publishes grants into a job ring that
+ * the running launch reads (completion is polled by copies; nothing waits
+ * for a launch to end), and the launch exits once every active job's trials
+ * are published and walked, so a busy period pays one launch tail.  While
+ * jobs are pending, call cmc_server_step at least every few seconds: the
+ * launch's wait for new work is bounded and reports CMC_ETIMEOUT past it. */
+int cmc_server_set_option(cmc_server* server, const char* name, double value);
 /* Device-time accounting of the iterations read back so far (CUDA events
  * around each engine launch): engine_ms sums the launches, busy_ms counts
  * time with at least one engine running once (pipelined iterations

@@ -39,7 +39,7 @@ EXPORTS = (
     "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats", "cmc_launch_static",
     "cmc_run_jobs", "cmc_autotune", "cmc_server_create", "cmc_server_submit", "cmc_server_step",
     "cmc_server_status", "cmc_server_pending", "cmc_server_error", "cmc_server_destroy",
-    "cmc_server_policy", "cmc_server_get_stats",
+    "cmc_server_policy", "cmc_server_get_stats", "cmc_server_set_option",
 )
 
 
@@ -145,6 +145,8 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.cmc_server_pending.restype = u32
     lib.cmc_server_get_stats.argtypes = [vp, vp]
     lib.cmc_server_get_stats.restype = ctypes.c_int
+    lib.cmc_server_set_option.argtypes = [vp, ctypes.c_char_p, ctypes.c_double]
+    lib.cmc_server_set_option.restype = ctypes.c_int
     lib.cmc_server_error.argtypes = [vp]
     lib.cmc_server_error.restype = ctypes.c_char_p
     lib.cmc_server_destroy.argtypes = [vp]
@@ -359,6 +361,11 @@ class Server:
         if rc:
             self._raise(rc)
         return {name: getattr(out, name) for name, _ in ServerStats._fields_}
+
+    def set_option(self, name: str, value: float) -> None:
+        rc = self.lib.cmc_server_set_option(self.handle, name.encode(), float(value))
+        if rc:
+            self._raise(rc)
 
     def policy(self, fifo_share: float) -> None:
         rc = self.lib.cmc_server_policy(self.handle, fifo_share)

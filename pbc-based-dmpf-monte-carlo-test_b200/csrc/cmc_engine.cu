@@ -40,6 +40,7 @@ struct GroupHeader {
     unsigned long long walk, rnd, shift, step;
     uint32_t slot, cand_next, abort, live;
     unsigned long long entry;  // resident launch: ring entry of the last trial
+    unsigned long long avail;  // resident launch: the last published end this group read
     Job jd;                    // this trial's job descriptor, read at L2
 };
 static_assert(sizeof(GroupHeader) <= kGroupHeaderBytes, "the planner reserves kGroupHeaderBytes");
@@ -90,6 +91,12 @@ __device__ __forceinline__ uint32_t ld_acquire_sys(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
 __device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
@@ -304,7 +311,10 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
     uint32_t cursor = 0;
     const unsigned long long total = a.total_dev ? *a.total_dev : a.total;
 
-    if (gt == 0) gh->entry = a.entry_begin;
+    if (gt == 0) {
+        gh->entry = a.entry_begin;
+        gh->avail = 0;
+    }
     for (;;) {
         if (gt == 0) {
             const unsigned long long gi = a.gidx_begin + atomicAdd(&a.ctrl->next, 1ULL);
@@ -316,17 +326,23 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
                 // closes the launch.  Claims rise, so a group that leaves
                 // holds an index past the final `avail`: every published
                 // trial is taken by some group.
-                live = 0;
-                uint32_t spins = 0;
-                for (;;) {
+                // The wait backs off from 1 to 128 us between reads of host
+                // memory (idle groups must not crowd the host's copies) and
+                // gives up after spin_limit microseconds.
+                live = gi < gh->avail;  // published as of this group's last read of host memory
+                uint32_t nap = 1024;
+                const unsigned long long t_start = globaltimer_ns();
+                while (!live) {
                     const uint32_t stop = ld_acquire_sys(&a.rq->stop);
-                    if (gi < ld_acquire_sys(&a.rq->avail)) {
+                    gh->avail = ld_acquire_sys(&a.rq->avail);
+                    if (gi < gh->avail) {
                         live = 1;
                         break;
                     }
                     if (stop) break;
-                    __nanosleep(1024);
-                    if (++spins > a.spin_limit) {
+                    __nanosleep(nap);
+                    nap = min(nap * 2, 131072u);
+                    if (globaltimer_ns() - t_start > 1000ULL * a.spin_limit) {
                         atomicExch(&a.ctrl->error, kErrTimeout);
                         atomicExch(&a.ctrl->where, 4u);
                         break;

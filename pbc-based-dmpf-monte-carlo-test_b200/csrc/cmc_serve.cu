@@ -1,32 +1,37 @@
 // cmc_serve.cu -- serving loop: estimation jobs of different sizes admitted as
 // they arrive and run together in the persistent engine (continuous batching).
 //
-// Each admitted job has a device-resident ServeState: its parameters, its RNG
-// counter (`next`, the index of its next trial), its budget and the cached key
-// of its current batch; its failure and trial counts accumulate on the device
-// (the engine's per-job counters, indexed by server slot).  One iteration
-// (`cmc_server_step`):
-//   1. admits queued jobs while their slot memory fits the device-memory budget;
-//   2. picks one size class (jobs whose walk slots fit in shared memory, or
-//      not) and grants its jobs trials: most of the step's work (95% by
-//      default) in arrival order, so no job starves and the tail stays that
-//      of plain per-job launches, the rest shortest remaining work first;
-//   3. the scheduler kernel turns the grants into the engine's job table on the
-//      device -- clamping at batch ends, deriving a batch key with device AES
-//      when a job enters a new batch, advancing the RNG counters, prefix-summing
-//      the table -- and writes the iteration's trial total to device memory;
-//   4. one engine launch runs every granted trial; the failure compaction
-//      follows; the host maps failures back to (job, batch, offset);
-//   5. finished batches are appended to the job's v3 journal (optional), and
-//      finished jobs free their slot.
-// A job's results are identical alone and in the mix: trial identity is
-// (seed, batch, offset) and does not depend on scheduling.
+// Admitted jobs keep their state on the device: per-job failure and trial
+// counts (the engine's counters, indexed by server slot) and, per published
+// grant, a job-table entry with the batch key, the first offset and the
+// count -- the job's RNG position (trial identity is (seed, batch, offset)).
+// The host grants trials: most of the work (95% by default) in arrival order,
+// so no job starves and the tail stays that of plain per-job launches, the
+// rest shortest remaining work first.  Two ways to run the grants:
+//
+//   resident (default): one engine launch stays on the device while jobs are
+//   pending.  The host writes grants into a job ring and publishes them
+//   through mapped host memory; the launch's producer groups pick them up as
+//   they claim trials; the host polls per-entry walk counts by copy and reads
+//   back finished entries' failure bits.  The launch exits once every active
+//   job's trials are published and walked: one launch tail per busy period.
+//
+//   iterations: each cmc_server_step issues one engine launch over one size
+//   class of jobs (shared or global walk slots), pipelined two deep on two
+//   streams; a device scheduler kernel turns the grants into the table,
+//   deriving batch keys with device AES and advancing device RNG counters.
+//
+// Finished batches are appended to the job's v3 journal (optional), and
+// finished jobs free their slot.  A job's results are identical alone and in
+// the mix: trial identity does not depend on scheduling.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <deque>
+#include <thread>
 #include <memory>
 #include <string>
 #include <vector>
@@ -187,6 +192,40 @@ struct Server {
     uint64_t fixed_bytes = 0;
     double fifo_share = 0.95;  // part of each step's work granted in arrival order
     std::string err;
+    unsigned long long* h_zero = nullptr;  // pinned zeros: counter resets by copy, never by kernel
+
+    // ---- resident mode: one engine launch stays on the device while work is
+    // published to it (see step_resident) ----
+    static constexpr uint32_t kRing = 4096;               // job-table ring entries
+    static constexpr uint64_t kRingBits = 1ULL << 24;     // failure-bitmap ring (trials in flight)
+    struct REntry {
+        uint32_t job, count, first;
+        uint64_t base, batch;
+        bool consumed;
+    };
+    bool resident = true;
+    bool r_ready = false, r_running = false, r_stopping = false;
+    std::deque<REntry> rlive;          // published entries not yet reclaimed; front = entry r_front
+    uint64_t r_front = 0, r_entries = 0;
+    uint64_t r_avail = 0;              // trials published (global index end)
+    uint64_t r_begin = 0;              // first trial of the running (or next) launch
+    Plan r_plan;
+    ResidentQueue* h_rq = nullptr;     // mapped pinned host memory
+    ResidentQueue* d_rq = nullptr;     // its device address
+    Job* d_ring = nullptr;
+    Job* h_ring = nullptr;             // pinned staging, one per ring entry
+    uint32_t* d_rdone = nullptr;
+    uint32_t* h_rdone = nullptr;       // pinned
+    uint32_t* d_rbits = nullptr;
+    uint32_t* h_rbits = nullptr;       // pinned mirror of the bitmap ring
+    Ctrl* d_rctrl = nullptr;
+    Ctrl* h_rctrl = nullptr;           // pinned
+    unsigned long long* h_rnext = nullptr;  // pinned: the running launch's claim counter
+    uint64_t r_claimed = 0;            // trials the running launch has claimed (at the last poll)
+    char* d_rpool = nullptr;
+    uint64_t rpool_bytes = 0;
+    cudaStream_t r_kstream = nullptr, r_cstream = nullptr;
+    cudaEvent_t r_e0 = nullptr, r_e1 = nullptr, r_kdone = nullptr;
 
     int fail(int code, const std::string& m) {
         err = m;
@@ -219,6 +258,24 @@ struct Server {
             if (b.e1) cudaEventDestroy(b.e1);
             if (b.stream) cudaStreamDestroy(b.stream);
         }
+        if (r_kstream) cudaStreamSynchronize(r_kstream);
+        if (r_cstream) cudaStreamSynchronize(r_cstream);
+        cudaFree(d_ring);
+        cudaFree(d_rdone);
+        cudaFree(d_rbits);
+        cudaFree(d_rctrl);
+        cudaFree(d_rpool);
+        cudaFreeHost(h_rq);
+        cudaFreeHost(h_ring);
+        cudaFreeHost(h_rdone);
+        cudaFreeHost(h_rbits);
+        cudaFreeHost(h_rctrl);
+        cudaFreeHost(h_rnext);
+        cudaFreeHost(h_zero);
+        for (cudaEvent_t e : {r_e0, r_e1, r_kdone})
+            if (e) cudaEventDestroy(e);
+        if (r_kstream) cudaStreamDestroy(r_kstream);
+        if (r_cstream) cudaStreamDestroy(r_cstream);
         if (origin) cudaEventDestroy(origin);
         cudaFree(d_states);
         cudaFreeHost(h_stage);
@@ -251,6 +308,8 @@ struct Server {
         const size_t words = (max_iter_trials + 31) / 32;
         if ((rc = alloc((void**)&d_states, sizeof(ServeState) * mj, "job states"))) return rc;
         if ((rc = host((void**)&h_stage, sizeof(ServeState) * mj, "job state staging"))) return rc;
+        if ((rc = host((void**)&h_zero, 64, "zeros"))) return rc;
+        std::memset(h_zero, 0, 64);
         if ((rc = alloc((void**)&d_failed, 8 * mj, "failure counters"))) return rc;
         if ((rc = alloc((void**)&d_done, 8 * mj, "trial counters"))) return rc;
         for (StepBuf& b : bufs) {
@@ -281,9 +340,11 @@ struct Server {
         if ((rc = cuda(cudaEventCreate(&origin), "event"))) return rc;
         if ((rc = cuda(cudaEventRecord(origin, bufs[0].stream), "event"))) return rc;
         if ((rc = cuda(cudaStreamSynchronize(bufs[0].stream), "init sync"))) return rc;
-        return cuda(cudaFuncSetAttribute((const void*)serve_schedule,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kTableBytes),
-                    "scheduler attribute");
+        if ((rc = cuda(cudaFuncSetAttribute((const void*)serve_schedule,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, kTableBytes),
+                       "scheduler attribute")))
+            return rc;
+        return resident ? resident_setup() : CMC_OK;  // the first step then allocates nothing
     }
 
     // Plan for a set of active parameter sets; returns the global pool bytes
@@ -421,8 +482,12 @@ struct Server {
             if ((rc = cuda(cudaMemcpyAsync(&d_states[j.slot], &h_stage[j.slot], sizeof state,
                                            cudaMemcpyHostToDevice, st), "upload job state")))
                 return rc;
-            if ((rc = cuda(cudaMemsetAsync(&d_failed[j.slot], 0, 8, st), "reset counter"))) return rc;
-            if ((rc = cuda(cudaMemsetAsync(&d_done[j.slot], 0, 8, st), "reset counter"))) return rc;
+            if ((rc = cuda(cudaMemcpyAsync(&d_failed[j.slot], h_zero, 8, cudaMemcpyHostToDevice, st),
+                           "reset counter")))
+                return rc;
+            if ((rc = cuda(cudaMemcpyAsync(&d_done[j.slot], h_zero, 8, cudaMemcpyHostToDevice, st),
+                           "reset counter")))
+                return rc;
         }
         return CMC_OK;
     }
@@ -434,6 +499,7 @@ struct Server {
         if (nfinished) *nfinished = 0;
         int rc = cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
         if (rc) return rc;
+        if (resident || r_running) return step_resident(work_blocks, finished, cap, nfinished);
         StepBuf& b = bufs[cur];
         StepBuf& prev = bufs[cur ^ 1];
         if (b.busy && (rc = process(b, finished, cap, nfinished))) return rc;  // not reached in order
@@ -458,6 +524,10 @@ struct Server {
     // Finishes every iteration in flight (used before the server goes away,
     // so journals hold every batch the device completed).
     int drain() {
+        if (r_ready) {
+            int rc = resident_close();
+            if (rc) return rc;
+        }
         for (int i = 0; i < 2; ++i) {
             StepBuf& b = bufs[(cur + i) & 1];  // oldest first
             if (b.busy) {
@@ -468,7 +538,8 @@ struct Server {
         return CMC_OK;
     }
 
-    int plan_grants(uint64_t work_blocks, std::vector<Grant>& grants, std::vector<uint32_t>& grant_jobs) {
+    int plan_grants(uint64_t work_blocks, std::vector<Grant>& grants, std::vector<uint32_t>& grant_jobs,
+                    bool one_class = true) {
         std::vector<uint32_t> all;  // active jobs with trials left to issue
         for (uint32_t id : active_ids())
             if (jobs[id].next < jobs[id].budget) all.push_back(id);
@@ -485,7 +556,7 @@ struct Server {
         const int cls = (iteration % 2 == 1) ? jobs[oldest].global_slots : jobs[smallest].global_slots;
         std::vector<uint32_t> ids;
         for (uint32_t id : all)
-            if (jobs[id].global_slots == cls) ids.push_back(id);
+            if (!one_class || jobs[id].global_slots == cls) ids.push_back(id);
         // grants: fifo_share of the work in arrival order (bounds the tail),
         // the rest shortest remaining work first (small jobs finish at once);
         // the step is at least 2.5x the latency of its slowest trial so that
@@ -731,6 +802,433 @@ struct Server {
         return CMC_OK;
     }
 
+    // ------------------------------------------------------------ resident --
+    //
+    // One engine launch stays on the device while jobs are served.  The host
+    // writes job entries (one per grant, batch key derived on the host) into
+    // a device ring by copy, waits for the copy, then raises `avail` in mapped
+    // host memory; producer groups claim trial indices, wait (bounded) until
+    // they are published, and find their entry by scanning the ring forward.
+    // Walkers count finished walks per entry; the host polls those counts by
+    // copy and reads the finished entries' failure bits.  When no active job
+    // has trials left to publish, the host raises `stop`: the launch finishes
+    // what was published and exits, so a busy period pays one launch tail (a
+    // plain launch pays one per job).  Nothing is queued on the device that
+    // needs an SM while the launch runs: counters and control words are reset
+    // by copies.
+
+    int resident_setup() {
+        if (r_ready) return CMC_OK;
+        auto alloc = [&](void** p, size_t bytes, const char* what) {
+            if (cudaMalloc(p, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(CMC_ENOMEM, std::string("cudaMalloc for ") + what);
+            }
+            return CMC_OK;
+        };
+        auto host = [&](void** p, size_t bytes, unsigned flags, const char* what) {
+            if (cudaHostAlloc(p, bytes, flags) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(CMC_ENOMEM, std::string("cudaHostAlloc for ") + what);
+            }
+            return CMC_OK;
+        };
+        int rc;
+        if ((rc = host((void**)&h_rq, sizeof(ResidentQueue), cudaHostAllocMapped, "resident queue"))) return rc;
+        std::memset(h_rq, 0, sizeof(ResidentQueue));
+        if ((rc = cuda(cudaHostGetDevicePointer((void**)&d_rq, h_rq, 0), "map resident queue"))) return rc;
+        if ((rc = alloc((void**)&d_ring, sizeof(Job) * kRing, "job ring"))) return rc;
+        if ((rc = host((void**)&h_ring, sizeof(Job) * kRing, cudaHostAllocDefault, "job ring staging"))) return rc;
+        if ((rc = alloc((void**)&d_rdone, 4 * kRing, "entry counts"))) return rc;
+        if ((rc = host((void**)&h_rdone, 4 * kRing, cudaHostAllocDefault, "entry counts"))) return rc;
+        if ((rc = alloc((void**)&d_rbits, kRingBits / 8, "bitmap ring"))) return rc;
+        if ((rc = host((void**)&h_rbits, kRingBits / 8, cudaHostAllocDefault, "bitmap ring"))) return rc;
+        if ((rc = alloc((void**)&d_rctrl, sizeof(Ctrl), "control block"))) return rc;
+        if ((rc = host((void**)&h_rctrl, sizeof(Ctrl), cudaHostAllocDefault, "control block"))) return rc;
+        if ((rc = host((void**)&h_rnext, 8, cudaHostAllocDefault, "claim counter"))) return rc;
+        if ((rc = cuda(cudaStreamCreateWithFlags(&r_kstream, cudaStreamNonBlocking), "stream"))) return rc;
+        if ((rc = cuda(cudaStreamCreateWithFlags(&r_cstream, cudaStreamNonBlocking), "stream"))) return rc;
+        if ((rc = cuda(cudaEventCreate(&r_e0), "event"))) return rc;
+        if ((rc = cuda(cudaEventCreate(&r_e1), "event"))) return rc;
+        if ((rc = cuda(cudaEventCreateWithFlags(&r_kdone, cudaEventDisableTiming), "event"))) return rc;
+        // no launch runs yet: plain memsets are fine here
+        if ((rc = cuda(cudaMemsetAsync(d_rbits, 0, kRingBits / 8, r_cstream), "memset"))) return rc;
+        if ((rc = cuda(cudaMemsetAsync(d_rdone, 0, 4 * kRing, r_cstream), "memset"))) return rc;
+        if ((rc = cuda(cudaStreamSynchronize(r_cstream), "resident setup"))) return rc;
+        r_ready = true;
+        return CMC_OK;
+    }
+
+    // Plan of a resident launch: global walk slots with four isolated walker
+    // warps (slot count does not depend on the table size), sized for every
+    // active and queued job.
+    int resident_plan(Plan& pl, uint64_t& pool) {
+        std::vector<uint32_t> ids = active_ids();
+        for (uint32_t id : queue) ids.push_back(id);
+        const uint32_t gs = ctx->force_global_slots, wk = ctx->force_walkers;
+        const int iso = ctx->force_isolate, wc = ctx->force_walker_ctas;
+        ctx->force_global_slots = 1;
+        ctx->force_isolate = 1;
+        ctx->force_walkers = 4;
+        ctx->force_walker_ctas = 0;
+        std::vector<Job> shapes;
+        const int rc = plan_for(ids, pl, shapes, pool);
+        ctx->force_global_slots = gs;
+        ctx->force_walkers = wk;
+        ctx->force_isolate = iso;
+        ctx->force_walker_ctas = wc;
+        return rc;
+    }
+
+    // Can job `id` run under the running launch's plan (slot size, entry width)?
+    bool fits(uint32_t id) {
+        Plan one;
+        uint64_t pool = 0;
+        std::vector<Job> shapes;
+        if (plan_for({id}, one, shapes, pool)) return false;
+        const uint32_t entry = r_plan.variant ? 4 : 2;
+        const Job& j = shapes[0];
+        const uint64_t bins = (uint64_t(j.buckets) * entry + 15) / 16 * 16;
+        const uint64_t map = (uint64_t(j.pnum) * j.k * entry + 15) / 16 * 16;
+        // the map of every slot starts at the plan's bins_bytes
+        return one.variant <= r_plan.variant && bins <= r_plan.bins_bytes &&
+               r_plan.bins_bytes + map <= r_plan.slot_stride;
+    }
+
+    // Published trials no producer has claimed yet, in AES-block equivalents:
+    // the work that keeps the running launch busy until the next publication.
+    double resident_unclaimed() const {
+        double w = 0;
+        for (const REntry& e : rlive) {
+            const uint64_t end = e.base + e.count;
+            if (end > r_claimed) w += double(end - std::max(e.base, r_claimed)) * jobs[e.job].cost;
+        }
+        return w;
+    }
+
+    // Publishes one chunk of grants (returns the number of entries published).
+    int resident_publish(uint64_t work_blocks, uint32_t& published) {
+        published = 0;
+        std::vector<Grant> grants;
+        std::vector<uint32_t> grant_jobs;
+        int rc = plan_grants(work_blocks, grants, grant_jobs, /*one_class=*/false);
+        if (rc) return rc;
+        size_t n = 0;
+        for (; n < grants.size(); ++n) {
+            const uint32_t id = grant_jobs[n];
+            const uint64_t bits_front = rlive.empty() ? r_avail : rlive.front().base;
+            const bool room = rlive.size() + 1 <= kRing && r_avail + grants[n].trials - bits_front <= kRingBits;
+            if (!room || (r_running && !fits(id))) break;
+            HostJob& j = jobs[id];
+            const uint64_t first_trial = j.next - grants[n].trials;  // plan_grants advanced next
+            const uint64_t per = 1ULL << j.bt;
+            REntry e{id, grants[n].trials, uint32_t(first_trial & (per - 1)), r_avail, first_trial >> j.bt, false};
+            Job& d = h_ring[r_entries % kRing];
+            if ((rc = ctx->make_job(j.params, e.first, e.count, e.base, d))) return fail(rc, ctx->err);
+            batch_key(j.seed, e.batch, d.batch_rk);
+            d.user = j.slot;
+            const uint32_t slot = uint32_t(r_entries % kRing);
+            if ((rc = cuda(cudaMemcpyAsync(&d_ring[slot], &d, sizeof(Job), cudaMemcpyHostToDevice, r_cstream),
+                           "publish entry")))
+                return rc;
+            if ((rc = cuda(cudaMemcpyAsync(&d_rdone[slot], h_zero, 4, cudaMemcpyHostToDevice, r_cstream),
+                           "publish entry")))
+                return rc;
+            rlive.push_back(e);
+            ++r_entries;
+            r_avail += e.count;
+            ++published;
+        }
+        // grants that did not fit go back to their jobs
+        for (size_t i = n; i < grants.size(); ++i) jobs[grant_jobs[i]].next -= grants[i].trials;
+        if (published) {
+            // the entries are in device memory before `avail` admits them
+            if ((rc = cuda(cudaStreamSynchronize(r_cstream), "publish"))) return rc;
+            __atomic_store_n(&h_rq->avail, (unsigned long long)r_avail, __ATOMIC_RELEASE);
+        }
+        if (n < grants.size() && r_running && !fits(grant_jobs[n])) {
+            // a larger table than the running plan holds: close this launch;
+            // the next one is planned for it
+            __atomic_store_n(&h_rq->stop, 1u, __ATOMIC_RELEASE);
+            r_stopping = true;
+        }
+        return CMC_OK;
+    }
+
+    int resident_launch() {
+        Plan pl;
+        uint64_t pool = 0;
+        int rc = resident_plan(pl, pool);
+        if (rc) return rc;
+        if (pool > rpool_bytes) {
+            cudaFree(d_rpool);
+            d_rpool = nullptr;
+            rpool_bytes = 0;
+            if (cudaMalloc((void**)&d_rpool, pool) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(CMC_ENOMEM, "resident slot pool");
+            }
+            rpool_bytes = pool;
+        }
+        // the entry holding the launch's first trial
+        uint64_t e_begin = r_front;
+        for (const REntry& e : rlive) {
+            if (r_begin >= e.base && r_begin - e.base < e.count) break;
+            ++e_begin;
+        }
+        if (e_begin == r_front + rlive.size()) return fail(CMC_EINVAL, "resident launch without published work");
+        __atomic_store_n(&h_rq->stop, 0u, __ATOMIC_RELEASE);
+        cudaStream_t st = r_kstream;
+        if ((rc = cuda(cudaMemcpyAsync(d_rctrl, h_zero, sizeof(Ctrl) <= 64 ? sizeof(Ctrl) : 64,
+                                       cudaMemcpyHostToDevice, st), "reset ctrl")))
+            return rc;
+        static_assert(sizeof(Ctrl) <= 64, "control block reset copies 64 zero bytes");
+        EngineArgs a{};
+        a.jobs = d_ring;
+        a.njobs = kRing;
+        a.total = ~0ULL;
+        a.gidx_begin = r_begin;
+        a.ctrl = d_rctrl;
+        a.fail_bits = d_rbits;
+        a.bits_mask = kRingBits - 1;
+        a.job_failed = d_failed;
+        a.job_done = d_done;
+        a.count_by_user = 1;
+        a.rq = d_rq;
+        a.ring_mask = kRing - 1;
+        a.entry_begin = e_begin;
+        a.entry_done = d_rdone;
+        a.gslots = pl.slots_smem ? nullptr : d_rpool;
+        a.gcache = pl.gcache_bytes ? reinterpret_cast<uint16_t*>(d_rpool + cache_offset(pl)) : nullptr;
+        a.gcache_stride = pl.gcache_stride;
+        a.t0 = ctx->d_t0;
+        a.slot_stride = pl.slot_stride;
+        a.bins_bytes = pl.bins_bytes;
+        a.ng = pl.ng;
+        a.wg = pl.wg;
+        a.ns = pl.ns;
+        a.nw = pl.nw;
+        a.isolate_walkers = pl.isolate;
+        a.r256 = 256u;
+        a.group_bytes = pl.group_bytes;
+        a.group_off = pl.group_off;
+        a.slots_off = pl.slots_off;
+        a.spin_limit = ctx->spin_limit;
+        const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
+                       : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
+                                         : (const void*)cmc_engine<uint32_t, uint32_t, true>;
+        if ((rc = cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(pl.smem_bytes)), "engine attribute")))
+            return rc;
+        void* args[] = {&a};
+        if ((rc = cuda(cudaEventRecord(r_e0, st), "event"))) return rc;
+        if ((rc = cuda(cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, st),
+                       "resident launch")))
+            return rc;
+        if ((rc = cuda(cudaEventRecord(r_e1, st), "event"))) return rc;
+        if ((rc = cuda(cudaMemcpyAsync(h_rctrl, d_rctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st), "read ctrl")))
+            return rc;
+        if ((rc = cuda(cudaEventRecord(r_kdone, st), "event"))) return rc;
+        r_plan = pl;
+        r_running = true;
+        r_stopping = false;
+        return CMC_OK;
+    }
+
+    // The launch has exited: check it and account its device time.
+    int resident_finished() {
+        int rc = cuda(cudaEventSynchronize(r_kdone), "resident sync");
+        if (rc) return rc;
+        r_running = false;
+        r_stopping = false;
+        r_begin = r_avail;  // every published trial was claimed and walked
+        if (h_rctrl->error)
+            return fail(-int(h_rctrl->error), "device wait gave up (site " + std::to_string(h_rctrl->where) +
+                                                  "): results discarded");
+        float t0 = 0, t1 = 0;
+        if ((rc = cuda(cudaEventElapsedTime(&t0, origin, r_e0), "engine timing"))) return rc;
+        if ((rc = cuda(cudaEventElapsedTime(&t1, origin, r_e1), "engine timing"))) return rc;
+        stats.iterations += 1;
+        stats.engine_ms += t1 - t0;
+        stats.busy_ms += std::max(0.0, double(t1) - std::max(double(t0), last_end_ms));
+        if (stats.iterations == 1) first_start_ms = t0;
+        last_end_ms = std::max(last_end_ms, double(t1));
+        stats.span_ms = last_end_ms - first_start_ms;
+        return CMC_OK;
+    }
+
+    // Reads finished entries back; returns how many entries it consumed.
+    int resident_poll(uint32_t& consumed) {
+        consumed = 0;
+        int rc;
+        if (r_running) {
+            if ((rc = cuda(cudaMemcpyAsync(h_rnext, &d_rctrl->next, 8, cudaMemcpyDeviceToHost, r_cstream),
+                           "poll")))
+                return rc;
+            if ((rc = cuda(cudaStreamSynchronize(r_cstream), "poll"))) return rc;
+            r_claimed = std::min<uint64_t>(r_begin + *h_rnext, r_avail);
+        } else {
+            r_claimed = r_begin;
+        }
+        if (rlive.empty()) return CMC_OK;
+        const uint32_t lo = uint32_t(r_front % kRing), n = uint32_t(rlive.size());
+        const uint32_t n1 = std::min(n, kRing - lo);
+        if ((rc = cuda(cudaMemcpyAsync(h_rdone + lo, d_rdone + lo, 4ULL * n1, cudaMemcpyDeviceToHost, r_cstream),
+                       "poll")))
+            return rc;
+        if (n > n1 && (rc = cuda(cudaMemcpyAsync(h_rdone, d_rdone, 4ULL * (n - n1), cudaMemcpyDeviceToHost,
+                                                 r_cstream), "poll")))
+            return rc;
+        if ((rc = cuda(cudaStreamSynchronize(r_cstream), "poll"))) return rc;
+        std::vector<size_t> ready;
+        for (size_t i = 0; i < rlive.size(); ++i) {
+            const REntry& e = rlive[i];
+            if (!e.consumed && h_rdone[(r_front + i) % kRing] >= e.count) ready.push_back(i);
+        }
+        if (ready.empty()) return CMC_OK;
+        // failure bits of the finished entries (word ranges of the bit ring)
+        const uint64_t words = kRingBits / 32;
+        for (size_t i : ready) {
+            const REntry& e = rlive[i];
+            uint64_t w0 = (e.base & (kRingBits - 1)) / 32;
+            uint64_t nw = (e.base % 32 + e.count + 31) / 32;
+            while (nw) {
+                const uint64_t take = std::min(nw, words - w0);
+                if ((rc = cuda(cudaMemcpyAsync(h_rbits + w0, d_rbits + w0, 4 * take, cudaMemcpyDeviceToHost,
+                                               r_cstream), "read failures")))
+                    return rc;
+                nw -= take;
+                w0 = 0;
+            }
+        }
+        if ((rc = cuda(cudaStreamSynchronize(r_cstream), "read failures"))) return rc;
+        for (size_t i : ready) {
+            REntry& e = rlive[i];
+            HostJob& j = jobs[e.job];
+            auto& pend = j.pending;
+            if (pend.empty() || pend.back().first != e.batch) {
+                // batches complete in order per job: insert keeping the list sorted
+                auto it = pend.begin();
+                while (it != pend.end() && it->first < e.batch) ++it;
+                if (it == pend.end() || it->first != e.batch) it = pend.insert(it, {e.batch, {}});
+                for (uint64_t g = e.base; g < e.base + e.count; ++g) {
+                    const uint64_t b = g & (kRingBits - 1);
+                    if (h_rbits[b >> 5] >> (b & 31) & 1u) {
+                        it->second.push_back(e.first + uint32_t(g - e.base));
+                        ++j.failed;
+                    }
+                }
+            } else {
+                for (uint64_t g = e.base; g < e.base + e.count; ++g) {
+                    const uint64_t b = g & (kRingBits - 1);
+                    if (h_rbits[b >> 5] >> (b & 31) & 1u) {
+                        pend.back().second.push_back(e.first + uint32_t(g - e.base));
+                        ++j.failed;
+                    }
+                }
+            }
+            j.processed += e.count;
+            stats.trials += e.count;
+            e.consumed = true;
+            ++consumed;
+        }
+        while (!rlive.empty() && rlive.front().consumed) {
+            rlive.pop_front();
+            ++r_front;
+        }
+        return CMC_OK;
+    }
+
+    // Commits complete batches and retires finished jobs.  A job's entries
+    // may finish out of order, so a batch is complete when every trial of it
+    // was read back: the job's processed count covers it only once all its
+    // earlier entries finished too, so completion is checked per batch from
+    // the entries still in flight.
+    int resident_commit(uint32_t* finished, uint32_t cap, uint32_t& nfin) {
+        std::vector<uint64_t> inflight_min(jobs.size(), ~0ULL);  // lowest unfinished trial per job
+        for (const REntry& e : rlive)
+            if (!e.consumed) {
+                const uint64_t t = (e.batch << jobs[e.job].bt) + e.first;
+                inflight_min[e.job] = std::min(inflight_min[e.job], t);
+            }
+        for (uint32_t id : active_ids()) {
+            HostJob& j = jobs[id];
+            const uint64_t per = 1ULL << j.bt;
+            const uint64_t done_upto = std::min(j.next, inflight_min[id]);  // every trial below is read back
+            while (!j.pending.empty()) {
+                const uint64_t bb = j.pending.front().first;
+                const uint64_t end = std::min<uint64_t>((bb + 1) << j.bt, j.budget);
+                if (done_upto < end) break;
+                auto& offs = j.pending.front().second;
+                std::sort(offs.begin(), offs.end());
+                if (j.journal) {
+                    try {
+                        j.journal->append(bb, uint32_t(std::min<uint64_t>(per, batch_length(j.jopt, bb))), offs);
+                    } catch (const std::exception& ex) {
+                        return fail(CMC_EINVAL, std::string("journal: ") + ex.what());
+                    }
+                }
+                j.pending.erase(j.pending.begin());
+            }
+            if (j.processed >= j.budget && j.pending.empty()) {
+                j.state = 2;
+                j.journal.reset();
+                free_slots.push_back(j.slot);
+                if (finished && nfin < cap) finished[nfin] = id;
+                ++nfin;
+            }
+        }
+        return CMC_OK;
+    }
+
+    int step_resident(uint64_t work_blocks, uint32_t* finished, uint32_t cap, uint32_t* nfinished) {
+        int rc = resident_setup();
+        if (rc) return rc;
+        if (r_running) {
+            const cudaError_t q = cudaEventQuery(r_kdone);
+            if (q == cudaSuccess) {
+                if ((rc = resident_finished())) return rc;
+            } else if (q != cudaErrorNotReady) {
+                return cuda(q, "resident launch");
+            }
+        }
+        uint32_t consumed = 0;
+        if ((rc = resident_poll(consumed))) return rc;
+        uint32_t nfin = 0;
+        if ((rc = resident_commit(finished, cap, nfin))) return rc;
+        if (nfinished) *nfinished = nfin;
+        if (!r_stopping && (rc = admit(r_cstream))) return rc;
+        // keep about two chunks of unclaimed work published ahead of the device
+        uint32_t published = 0;
+        if (!r_stopping && resident_unclaimed() < 2.0 * double(work_blocks) &&
+            (rc = resident_publish(work_blocks, published)))
+            return rc;
+        if (!r_running && r_avail > r_begin && (rc = resident_launch())) return rc;
+        // nothing left to publish: close the launch once it has the last work
+        bool more = !queue.empty();
+        for (uint32_t id : active_ids()) more = more || jobs[id].next < jobs[id].budget;
+        if (r_running && !r_stopping && !more) {
+            __atomic_store_n(&h_rq->stop, 1u, __ATOMIC_RELEASE);
+            r_stopping = true;
+        }
+        if (!published && !consumed && !nfin)
+            std::this_thread::sleep_for(std::chrono::microseconds(50));  // nothing moved: poll gently
+        return CMC_OK;
+    }
+
+    // Publishes nothing more, lets the launch finish, reads everything back.
+    int resident_close() {
+        if (r_running && !r_stopping) {
+            __atomic_store_n(&h_rq->stop, 1u, __ATOMIC_RELEASE);
+            r_stopping = true;
+        }
+        int rc;
+        if (r_running && (rc = resident_finished())) return rc;
+        uint32_t consumed = 0, nfin = 0;
+        if ((rc = resident_poll(consumed))) return rc;
+        return resident_commit(nullptr, 0, nfin);
+    }
+
     int status(uint32_t id, uint64_t* done, uint64_t* failed, int* state) {
         if (id >= jobs.size()) return fail(CMC_EINVAL, "unknown job id");
         HostJob& j = jobs[id];
@@ -787,6 +1285,21 @@ int cmc_server_status(cmc_server* server, uint32_t job_id, uint64_t* out_trials_
 int cmc_server_policy(cmc_server* server, double fifo_share) {
     if (!server || !(fifo_share >= 0.0 && fifo_share <= 1.0)) return CMC_EINVAL;
     reinterpret_cast<Server*>(server)->fifo_share = fifo_share;
+    return CMC_OK;
+}
+
+int cmc_server_set_option(cmc_server* server, const char* name, double value) {
+    if (!server || !name) return CMC_EINVAL;
+    Server* s = reinterpret_cast<Server*>(server);
+    const std::string n(name);
+    if (n == "fifo_share" && value >= 0.0 && value <= 1.0) {
+        s->fifo_share = value;
+    } else if (n == "resident" && (value == 0.0 || value == 1.0)) {
+        s->resident = value != 0.0;
+    } else {
+        s->err = "unknown server option or value: " + n;
+        return CMC_EINVAL;
+    }
     return CMC_OK;
 }
 

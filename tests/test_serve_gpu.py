@@ -28,9 +28,11 @@ def make_jobs(cmc, n, seed):
     return jobs
 
 
-def test_served_equals_alone(ctx, cmc, tmp_path):
+@pytest.mark.parametrize("resident", [0, 1])
+def test_served_equals_alone(ctx, cmc, tmp_path, resident):
     bt = 10
     srv = cmc.Server(ctx, max_jobs=16, mem_budget=1 << 30, batch_bits=bt, max_iteration_trials=1 << 16)
+    srv.set_option("resident", resident)
     jobs = make_jobs(cmc, 14, 3)
     ids = []
     finished = set()
@@ -60,17 +62,20 @@ def test_served_equals_alone(ctx, cmc, tmp_path):
     srv.close()
 
 
-def test_served_job_resumes_from_journal(ctx, cmc, tmp_path):
+@pytest.mark.parametrize("resident", [0, 1])
+def test_served_job_resumes_from_journal(ctx, cmc, tmp_path, resident):
     p = cmc.parameters("bgh25", 64, 16, 3, 70, 20, "affine")
     seed, budget, bt = 77, 4096, 8            # 16 batches of 256
     d = str(tmp_path / "j")
     srv = cmc.Server(ctx, max_jobs=4, batch_bits=bt, max_iteration_trials=1 << 12)
+    srv.set_option("resident", resident)
     srv.submit(p, seed, budget, d)
     srv.step(3 * 256 * 800)                   # a few batches only
     srv.close()
     part = cmc.read_journal(tmp_path / "j" / "worker_0.bin")
     assert 0 < len(part) < 16
     srv = cmc.Server(ctx, max_jobs=4, batch_bits=bt, max_iteration_trials=1 << 12)
+    srv.set_option("resident", resident)
     job = srv.submit(p, seed, budget, d)
     while srv.pending():
         srv.step(1 << 22)
@@ -78,3 +83,28 @@ def test_served_job_resumes_from_journal(ctx, cmc, tmp_path):
     assert full == alone(ctx, cmc, p, seed, budget, bt)
     assert srv.status(job)[2] == 2
     srv.close()
+
+
+def test_resident_larger_table_relaunches(ctx, cmc):
+    # a job whose walk slots exceed the running launch's plan closes that
+    # launch and runs in the next one; results stay those of the job alone
+    srv = cmc.Server(ctx, max_jobs=8, mem_budget=1 << 31, batch_bits=12, max_iteration_trials=1 << 16)
+    srv.set_option("resident", 1)
+    small = cmc.parameters("bgh25", 64, 16, 3, 80, 50, "affine")
+    big = cmc.parameters("bgh25", 3000, 24, 3, 3900, 100, "affine")
+    a = srv.submit(small, 3, 4096)
+    srv.step(1 << 20)
+    b = srv.submit(big, 4, 300)
+    steps = 0
+    while srv.pending():
+        srv.step(1 << 20)
+        steps += 1
+        assert steps < 100000
+    assert srv.status(a)[1] == len(alone_flat(ctx, cmc, small, 3, 4096, 12))
+    assert srv.status(b)[1] == len(alone_flat(ctx, cmc, big, 4, 300, 9))
+    assert srv.stats()["iterations"] >= 1
+    srv.close()
+
+
+def alone_flat(ctx, cmc, p, seed, budget, bt):
+    return [x for v in alone(ctx, cmc, p, seed, budget, bt).values() for x in v]
