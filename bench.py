@@ -30,10 +30,23 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 PKG_DIR = ROOT / "pbc-based-dmpf-monte-carlo-test_b200"
 
-WORKLOAD = dict(workload="plain GPU: N=2^20 keys, t=1024, k=3, B=1536, kick=500, bgh25, "
-                         "affine inputs, seed 2, batches of 2^20 trials",
-                mode="bgh25", input_mode="affine", pnum=1024, ell_i=20, k=3, buckets=1536,
-                kick=500, seed=2, bt=20)
+# Single-configuration workloads (one launch per step over one batch's trials).
+WORKLOADS = {
+    "config2": dict(workload="plain GPU: N=2^20 keys, t=1024, k=3, B=1536, kick=500, bgh25, "
+                             "affine inputs, seed 2, batches of 2^20 trials",
+                    mode="bgh25", input_mode="affine", pnum=1024, ell_i=20, k=3, buckets=1536,
+                    kick=500, seed=2, bt=20, trials=1 << 20),
+    "config1": dict(workload="plain method: N=2^16 keys, t=64, k=3, B=96, kick=100, bgh25, "
+                             "affine inputs, seed 1, batches of 2^16 trials",
+                    mode="bgh25", input_mode="affine", pnum=64, ell_i=16, k=3, buckets=96,
+                    kick=100, seed=1, bt=16, trials=1 << 16),
+    "config4": dict(workload="large table: N=2^28 keys, t=16384, k=3, B=24576, kick=1000, bgh25, "
+                             "affine inputs, seed 4, batches of 2^24 trials (first 2^16 of each "
+                             "per step)",
+                    mode="bgh25", input_mode="affine", pnum=16384, ell_i=28, k=3, buckets=24576,
+                    kick=1000, seed=4, bt=24, trials=1 << 16),
+}
+WORKLOAD = WORKLOADS["config2"]
 METRIC = "trials/s per B200 (bit-exact failures)"
 AES_BYTES_PER_BLOCK = 640      # 160 table lookups x 4 bytes
 SMEM_BYTES_PER_CLK_PER_SM = 128
@@ -116,9 +129,9 @@ def read_peaks() -> dict:
         return {}
 
 
-def read_traffic() -> float | None:
+def read_traffic(name: str = "config2") -> float | None:
     """DRAM bytes per engine launch from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / "engine_config2_traffic.txt"
+    f = ROOT / "profiles" / f"engine_{name}_traffic.txt"
     try:
         for line in f.read_text().splitlines():
             if line.startswith("dram_bytes_per_launch"):
@@ -151,11 +164,10 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
-def cpu_run(n_trials: int, batch: int, threads: int):
+def cpu_run(n_trials: int, batch: int, threads: int, w: dict = WORKLOAD):
     """Trials [0, n) of `batch` on the CPU: the reference's own cpu_batch_launch
     (oracle/_ref) when built here, else the oracle restatement.  Returns
     (seconds, kind, failures)."""
-    w = WORKLOAD
     lib = reference_lib()
     out = (ctypes.c_uint32 * max(n_trials, 1))()
     t0 = time.perf_counter()
@@ -176,37 +188,58 @@ def cpu_run(n_trials: int, batch: int, threads: int):
     return time.perf_counter() - t0, kind, n
 
 
-def cpu_sample_size(threads: int, target_seconds: float) -> tuple[int, float, str]:
+def cpu_sample_size(threads: int, target_seconds: float, w: dict = WORKLOAD) -> tuple[int, float, str]:
     """Grow the sample until one run takes about target_seconds (cap 2^20)."""
-    n = max(256, threads * 16)
+    n = max(256, threads * 16) if w["pnum"] < 4096 else threads * 2
     while True:
-        secs, kind, _ = cpu_run(n, 0, threads)
+        secs, kind, _ = cpu_run(n, 0, threads, w)
         if secs >= target_seconds * 0.5 or n >= 1 << 20:
             return n, secs, kind
         n = int(min(1 << 20, max(2 * n, n * target_seconds / max(secs, 1e-3))))
 
 
-def cpu_baseline(target_seconds: float = 10.0) -> dict:
+def cpu_baseline(target_seconds: float = 10.0, w: dict = WORKLOAD) -> dict:
     threads = host_threads()
-    n, secs, kind = cpu_sample_size(threads, target_seconds)
+    n, secs, kind = cpu_sample_size(threads, target_seconds, w)
     return {"value": n / secs, "unit": "trials/s", "cores": threads, "kind": kind,
             "sample": f"first {n} trials of batch 0 of the bench workload "
                       f"({'reference cpu_batch_launch, AES-NI' if kind == 'reference' else 'oracle port'}, "
                       f"{threads} threads, {secs:.1f} s)"}
 
 
+# ------------------------------------------------------------- replicas --
+
+def batch_of(step: int, rank: int, world: int) -> int:
+    """Batch id of rank `rank`'s step: ranks interleave, so every rank runs
+    disjoint batches of the same experiment (replicas, no collective on the
+    data path; the reference's workers claim batch ids the same way,
+    cuckoo_bench.cu:976)."""
+    return rank + world * step
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The slowest rank's time: whole-job throughput is set by it."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference_arm(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     threads = host_threads()
-    w = WORKLOAD
+    w = WORKLOADS.get(args.workload, WORKLOAD)
     # bounded sample per step: about 2 s of CPU work each
-    per_step, _, kind = cpu_sample_size(threads, 2.0)
+    per_step, _, kind = cpu_sample_size(threads, 2.0, w)
     for s in range(args.warmup):
-        cpu_run(per_step, s, threads)
+        cpu_run(per_step, s, threads, w)
     total = 0.0
     for s in range(args.steps):
-        secs, kind, _ = cpu_run(per_step, args.warmup + s, threads)
+        secs, kind, _ = cpu_run(per_step, args.warmup + s, threads, w)
         total += secs
     value = per_step * args.steps / total
     line = {
@@ -418,9 +451,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--trials", type=int, default=1 << 20,
-                    help="trials per step (default one batch, 2^20); smaller for profiling")
-    ap.add_argument("--workload", choices=["config2", "sweep", "serve"], default="config2")
+    ap.add_argument("--trials", type=int, default=0,
+                    help="trials per step (default: the workload's, 2^20 for config2); "
+                         "smaller for profiling")
+    ap.add_argument("--workload", choices=["config2", "config1", "config4", "sweep", "serve"],
+                    default="config2")
     ap.add_argument("--serve-jobs", type=int, default=400)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-log2-budget", default="10,16")
@@ -457,10 +492,10 @@ def main():
     torch.cuda.set_device(local)
     cmc = load_pkg()
     ctx = cmc.Context(local)
-    w = WORKLOAD
+    w = WORKLOADS[args.workload]
     p = cmc.parameters(w["mode"], w["pnum"], w["ell_i"], w["k"], w["buckets"], w["kick"],
                        w["input_mode"])
-    n = min(args.trials, 1 << w["bt"])
+    n = min(args.trials or w["trials"], 1 << w["bt"])
     # a dedicated stream: the legacy default stream's handle is NULL, which the
     # C ABI reads as "the context's own stream"
     stream = torch.cuda.Stream()
@@ -478,12 +513,9 @@ def main():
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
-    def batch_of(step):
-        return rank + world * step
-
     # warm-up (untimed)
     for s in range(args.warmup):
-        ctx.launch_device(p, key_of(batch_of(s)).data_ptr(), 0, n, d_out.data_ptr(),
+        ctx.launch_device(p, key_of(batch_of(s, rank, world)).data_ptr(), 0, n, d_out.data_ptr(),
                           d_n.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
     ctx.check()
@@ -491,7 +523,7 @@ def main():
     # timed region: K steps, per-step events on the launching stream, L2 flushed between
     steps = list(range(args.warmup, args.warmup + args.steps))
     for s in steps:
-        key_of(batch_of(s))
+        key_of(batch_of(s, rank, world))
     starts = [torch.cuda.Event(enable_timing=True) for _ in steps]
     ends = [torch.cuda.Event(enable_timing=True) for _ in steps]
     engine_ms = []
@@ -503,7 +535,7 @@ def main():
         for i, s in enumerate(steps):
             flush.zero_()
             starts[i].record(stream)
-            ctx.launch_device(p, key_of(batch_of(s)).data_ptr(), 0, n, d_out.data_ptr(),
+            ctx.launch_device(p, key_of(batch_of(s, rank, world)).data_ptr(), 0, n, d_out.data_ptr(),
                               d_n.data_ptr(), stream.cuda_stream)
             ends[i].record(stream)
             engine_ms.append(ctx.last_engine_ms())
@@ -515,15 +547,12 @@ def main():
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = sum(step_ms)
     launches = ctx.last_kernel_count * len(steps)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(total_ms, world, "cuda")
     value = world * n * len(steps) / (max_ms / 1e3)
 
     # e2e: the C ABI call with host buffers, copies inside the timed region
     e2e_steps = list(range(args.warmup + args.steps, args.warmup + 2 * args.steps))
-    host_keys = {s: cmc.batch_key(w["seed"], batch_of(s)) for s in e2e_steps}
+    host_keys = {s: cmc.batch_key(w["seed"], batch_of(s, rank, world)) for s in e2e_steps}
     ctx.launch(p, host_keys[e2e_steps[0]], 0, n)  # warm host path
     if world > 1:
         dist.barrier()
@@ -537,10 +566,8 @@ def main():
         d2h += 4 + 4 * len(fails)
     e1.record(stream)
     torch.cuda.synchronize()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * len(e2e_steps) / (float(t.item()) / 1e3)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
+    e2e_value = world * n * len(e2e_steps) / (e2e_ms / 1e3)
 
     if rank == 0:
         peaks = read_peaks()
@@ -551,7 +578,7 @@ def main():
         sms = torch.cuda.get_device_properties(local).multi_processor_count
         max_mhz = peaks.get("sm_max_mhz") or clk.get("sm_max_mhz") or 1965.0
         peak = sms * SMEM_BYTES_PER_CLK_PER_SM * max_mhz * 1e6 / 1e9
-        traffic = read_traffic()
+        traffic = read_traffic(args.workload)
         line = {
             "metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": world,
             "steps": len(steps), "warmup": args.warmup, "ms_per_step": max_ms / len(steps),
@@ -575,7 +602,7 @@ def main():
             "clocks": clk,
         }
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline()
+            line["cpu_baseline"] = cpu_baseline(w=w)
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
