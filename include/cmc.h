@@ -188,11 +188,14 @@ int cmc_server_destroy(cmc_server* server);
  * PRP half width h <= 12, else in global memory, 2 round cache in global
  * memory, L2-resident, for any h <= 16), "walkers"
  * (1..4 walker warps), "isolate_walkers" (-1 auto, 0/1: walker warps alone
- * on SM sub-partition 3, producers on 0..2), "slots_per_group" (cap on shared-memory slots per
- * group, default 8), "walker_ctas" (-1 auto, 0 walks inside each CTA, N > 0
- * dedicates N CTAs -- one per SM -- to walks over global slots while the
- * others only build maps), "spin_limit" (polls before a device wait gives up).  Returns CMC_EINVAL for an unknown
- * name or a value out of range. */
+ * on SM sub-partition 3, producers on 0..2), "slots_per_group" (cap on
+ * shared-memory slots per group, default 8), "walker_ctas" (-1 auto, 0 walks
+ * inside each CTA, N > 0 dedicates N CTAs -- one per SM -- to walks over
+ * global slots while the others only build maps), "spin_limit" (polls before
+ * a device wait gives up), "graph" (1, the default: cmc_run_jobs captures the
+ * device side of a call shape -- job shapes, counts and buffers -- into a CUDA
+ * graph on its second call and replays it from the third; 0: always eager).
+ * Returns CMC_EINVAL for an unknown name or a value out of range. */
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
 
 /* No counterpart in the reference.  The Launch seam for callers that cannot

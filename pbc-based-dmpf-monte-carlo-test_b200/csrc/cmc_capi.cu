@@ -339,10 +339,6 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
                 : (pl.variant == 0   ? (const void*)cmc_engine<uint16_t, uint16_t, false>
                    : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
                                      : (const void*)cmc_engine<uint32_t, uint32_t, true>);
-        if ((rc = cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(pl.smem_bytes)),
-                       "cudaFuncSetAttribute")))
-            return rc;
         void* args[] = {&a};
         // The split engine's producer and walker CTAs hand trials to each other, so
         // they must all be resident at once: a cooperative launch guarantees it.
@@ -390,6 +386,22 @@ int Ctx::check_ctrl() {
     return CMC_OK;
 }
 
+// Every engine kernel may use up to the device's opt-in shared memory.  Set
+// once per device and never lowered, so launches of different plans -- and
+// graphs captured from them -- are valid whatever ran in between.
+int engine_smem_cap(size_t optin) {
+    const void* fns[] = {(const void*)cmc_engine<uint16_t, uint16_t, false>,
+                         (const void*)cmc_engine<uint32_t, uint32_t, false>,
+                         (const void*)cmc_engine<uint32_t, uint32_t, true>,
+                         (const void*)cmc_engine_split<uint16_t, uint16_t, false>,
+                         (const void*)cmc_engine_split<uint32_t, uint32_t, false>,
+                         (const void*)cmc_engine_split<uint32_t, uint32_t, true>};
+    for (const void* fn : fns)
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(optin)) != cudaSuccess)
+            return CMC_ECUDA;
+    return CMC_OK;
+}
+
 int Ctx::init(int dev) {
     device = dev;
     int rc = cuda(cudaSetDevice(dev), "cudaSetDevice");
@@ -401,6 +413,10 @@ int Ctx::init(int dev) {
                     prop.major, prop.minor);
     sms = prop.multiProcessorCount;
     smem_optin = prop.sharedMemPerBlockOptin;
+    if (engine_smem_cap(smem_optin)) {
+        cudaGetLastError();
+        return fail(CMC_ECUDA, "cudaFuncSetAttribute on the engine kernels failed");
+    }
     if ((rc = cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream"))) return rc;
     if ((rc = cuda(cudaEventCreate(&ev_start), "event"))) return rc;
     if ((rc = cuda(cudaEventCreate(&ev_stop), "event"))) return rc;
@@ -443,6 +459,9 @@ Ctx::~Ctx() {
     cudaFree(d_ghdr);
     cudaFree(d_job_failed);
     cudaFree(d_key);
+    for (GraphEntry& g : graphs) cudaGraphExecDestroy(g.exec);
+    cudaFreeHost(h_failed);
+    cudaFreeHost(h_nf);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
     if (stream) cudaStreamDestroy(stream);
@@ -529,6 +548,26 @@ std::string Ctx::mix_key(const cmc_job* in, uint32_t n) const {
     std::string key;
     for (auto& x : parts) key += x + ";";
     return key;
+}
+
+// Everything a captured batched call bakes in: job shapes and counts in table
+// order, plan classes, planner options and the device buffers it touches.
+std::string Ctx::graph_key(const std::vector<Job>& jobs, const std::vector<uint32_t>& bounds,
+                           uint64_t total, uint64_t dev_cap) const {
+    std::string key;
+    char b[160];
+    for (const Job& j : jobs) {
+        snprintf(b, sizeof b, "%u/%u/%u/%u/%u/%u/%u/%u/%llu/%u;", j.mode, j.input_mode, j.pnum, j.k,
+                 j.buckets, j.kick, j.half_bits, j.method, (unsigned long long)j.domain, j.count);
+        key += b;
+    }
+    for (uint32_t x : bounds) key += std::to_string(x) + ",";
+    snprintf(b, sizeof b, "|%llu|%llu|%u/%u/%u/%u/%u/%d/%d/%d/%u|%p/%p/%p/%p/%p/%p/%p/%p",
+             (unsigned long long)total, (unsigned long long)dev_cap, force_wg, force_ng,
+             force_global_slots, force_walkers, max_slots_per_group, force_walker_ctas, force_isolate,
+             force_method, spin_limit, (void*)d_jobs, (void*)d_bits, (void*)d_out, (void*)d_slots,
+             (void*)d_ctrl, (void*)d_job_failed, (void*)h_failed, (void*)h_nf);
+    return key + b;
 }
 
 int Ctx::prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::vector<Job>& out,
@@ -636,21 +675,92 @@ int Ctx::run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t*
     cudaStream_t st = user_stream ? user_stream : stream;
     if ((rc = upload_jobs(jobs, st))) return rc;
     if ((rc = grow(d_job_failed, job_failed_cap, n, "job counters"))) return rc;
-    if ((rc = cuda(cudaMemsetAsync(d_job_failed, 0, n * sizeof(unsigned long long), st), "memset counters")))
-        return rc;
     const uint64_t dev_cap = out_offsets ? std::min<uint64_t>(cap, total) : 0;
     if ((rc = grow(d_out, out_cap, size_t(dev_cap) + 1, "failure list"))) return rc;
-    if ((rc = run(jobs, total, st, 0, d_out, d_out + dev_cap, dev_cap, d_job_failed, nullptr, &bounds)))
+    if (h_failed_cap < n) {
+        cudaFreeHost(h_failed);
+        h_failed = nullptr;
+        h_failed_cap = 0;
+        if (cudaHostAlloc((void**)&h_failed, n * sizeof(unsigned long long), cudaHostAllocDefault) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return fail(CMC_ENOMEM, "pinned job counters");
+        }
+        h_failed_cap = n;
+    }
+    if (!h_nf && cudaHostAlloc((void**)&h_nf, 4, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CMC_ENOMEM, "pinned count");
+    }
+    // The device side of the call: counters, the engine launches, the
+    // compaction and the read-back into pinned memory.
+    auto enqueue = [&]() -> int {
+        int r = cuda(cudaMemsetAsync(d_job_failed, 0, n * sizeof(unsigned long long), st), "memset counters");
+        if (r) return r;
+        if ((r = run(jobs, total, st, 0, d_out, d_out + dev_cap, dev_cap, d_job_failed, nullptr, &bounds)))
+            return r;
+        if ((r = cuda(cudaMemcpyAsync(h_failed, d_job_failed, n * sizeof(unsigned long long),
+                                      cudaMemcpyDeviceToHost, st), "read counters")))
+            return r;
+        return cuda(cudaMemcpyAsync(h_nf, d_out + dev_cap, 4, cudaMemcpyDeviceToHost, st), "read count");
+    };
+    // A call shape seen before is captured into a CUDA graph on its second
+    // call and replayed from the third: the job table is uploaded by copy
+    // first, everything else is one graph launch.  The first call runs eagerly
+    // so that buffers are sized and kernel attributes set before any capture.
+    graph_state = "eager";
+    if (use_graphs && force_walker_ctas <= 0) {
+        const std::string key = graph_key(jobs, bounds, total, dev_cap);
+        auto it = std::find_if(graphs.begin(), graphs.end(), [&](const GraphEntry& g) { return g.key == key; });
+        if (it != graphs.end()) {
+            if ((rc = cuda(cudaGraphLaunch(it->exec, st), "graph launch"))) return rc;
+            kernels = it->kernels;
+            ctrl_count = it->ctrl_count;
+            plan_text = it->plan_text;
+            last_plan = it->plan;
+            graph_state = "replayed";
+        } else if (std::find(graph_seen.begin(), graph_seen.end(), key) != graph_seen.end()) {
+            cudaGraph_t g = nullptr;
+            capturing = true;
+            rc = cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+            if (!rc) rc = enqueue();
+            const cudaError_t e = cudaStreamEndCapture(st, &g);
+            capturing = false;
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t ie = (!rc && e == cudaSuccess && g) ? cudaGraphInstantiate(&ex, g, 0)
+                                                                  : cudaErrorUnknown;
+            if (ie == cudaSuccess) {
+                if (graphs.size() >= 8) {
+                    cudaGraphExecDestroy(graphs.front().exec);
+                    graphs.erase(graphs.begin());
+                }
+                graphs.push_back(GraphEntry{key, ex, kernels, ctrl_count, plan_text, last_plan});
+                if (g) cudaGraphDestroy(g);
+                if ((rc = cuda(cudaGraphLaunch(ex, st), "graph launch"))) return rc;
+                graph_state = "captured";
+            } else {
+                // the shape could not be captured: run it eagerly
+                const std::string why = rc ? err
+                                      : std::string(cudaGetErrorName(e != cudaSuccess ? e : ie));
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                if ((rc = enqueue())) return rc;
+                graph_state = "eager(capture failed: " + why + ")";
+            }
+        } else {
+            if ((rc = enqueue())) return rc;
+            // keyed by the buffers as this call left them (it may have grown some)
+            graph_seen.push_back(graph_key(jobs, bounds, total, dev_cap));
+            if (graph_seen.size() > 64) graph_seen.erase(graph_seen.begin());
+        }
+    } else if ((rc = enqueue())) {
         return rc;
-    std::vector<unsigned long long> failed(n);
-    uint32_t nf = 0;
-    if ((rc = cuda(cudaMemcpyAsync(failed.data(), d_job_failed, n * sizeof(unsigned long long),
-                                   cudaMemcpyDeviceToHost, st), "read counters")))
-        return rc;
-    if ((rc = cuda(cudaMemcpyAsync(&nf, d_out + dev_cap, 4, cudaMemcpyDeviceToHost, st), "read count")))
-        return rc;
+    }
+    if (use_graphs) plan_text += " graph=" + graph_state;
     if ((rc = cuda(cudaStreamSynchronize(st), "batched sync"))) return rc;
     if ((rc = check_ctrl())) return rc;
+    std::vector<unsigned long long> failed(h_failed, h_failed + n);
+    const uint32_t nf = *h_nf;
     uint64_t sum = 0;
     for (uint32_t i = 0; i < n; ++i) {
         out_failed[order[i]] = failed[i];
@@ -814,6 +924,7 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "groups" && value >= 0 && value <= cmc::kMaxGroups) c->force_ng = uint32_t(value);
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
     else if (n == "method" && value >= -1 && value <= 2) c->force_method = int(value);
+    else if (n == "graph" && (value == 0 || value == 1)) c->use_graphs = int(value);
     else if (n == "walkers" && value >= 0 && value <= 4) c->force_walkers = uint32_t(value);
     else if (n == "isolate_walkers" && value >= -1 && value <= 1) c->force_isolate = int(value);
     else if (n == "walker_ctas" && value >= -1 && value < c->sms) c->force_walker_ctas = int(value);

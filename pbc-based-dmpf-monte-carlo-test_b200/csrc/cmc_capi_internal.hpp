@@ -28,6 +28,8 @@ struct Plan {
 };
 
 uint32_t choose_method(uint32_t h, uint64_t domain, double candidates, int force, bool may_allocate);
+// Raises the engine kernels' dynamic shared-memory limit to the device's opt-in maximum.
+int engine_smem_cap(size_t optin);
 // Estimated cost of one trial in AES-block equivalents (seeds, map, 0.1 t for the walk).
 double job_cost(const Job& j);
 
@@ -72,6 +74,22 @@ struct Ctx {
     uint32_t max_slots_per_group = 8;
     int force_walker_ctas = -1;  // -1 auto, 0 in-SM walker, N split engine
     int force_isolate = -1;      // -1 auto, 0 contiguous warp roles, 1 isolated walkers
+    // batched calls: captured CUDA graphs of the device side, by call shape
+    struct GraphEntry {
+        std::string key;
+        cudaGraphExec_t exec = nullptr;
+        uint32_t kernels = 0, ctrl_count = 1;
+        std::string plan_text;
+        Plan plan;
+    };
+    int use_graphs = 1;
+    bool capturing = false;
+    std::vector<GraphEntry> graphs;  // most recent last, at most 8
+    std::vector<std::string> graph_seen;
+    unsigned long long* h_failed = nullptr;  // pinned per-job counts of the last batched call
+    size_t h_failed_cap = 0;
+    uint32_t* h_nf = nullptr;                // pinned failure count of the last batched call
+    std::string graph_state;                 // "eager", "captured" or "replayed"
     int force_method = -1;  // -1 auto, 0 direct, 1 cache (shared if h <= 12, else global), 2 global cache
     bool may_allocate = true;  // false: no global round cache, global slots only if unavoidable
     uint32_t spin_limit = 1u << 26;
@@ -96,6 +114,8 @@ struct Ctx {
     int prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::vector<Job>& out,
                      std::vector<uint32_t>& order, uint64_t& total, std::vector<uint32_t>& bounds);
     std::string mix_key(const cmc_job* in, uint32_t n) const;
+    std::string graph_key(const std::vector<Job>& jobs, const std::vector<uint32_t>& bounds,
+                          uint64_t total, uint64_t dev_cap) const;
     int run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t* out_offsets,
                  uint32_t* out_jobs, uint64_t cap, uint64_t* out_total);
     int autotune(const cmc_job* in, uint32_t n, uint32_t sample_div);

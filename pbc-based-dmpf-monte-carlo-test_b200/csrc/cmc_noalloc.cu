@@ -124,6 +124,11 @@ int setup(int device, DeviceState*& out) {
         cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess)
         return fail(CMC_ECUDA, "cudaDeviceGetAttribute failed");
     if (major < 10) return fail(CMC_EINVAL, "cmc_launch_static needs an sm_100 device");
+    // the device maximum, the same value every caller sets (never lowered)
+    if (engine_smem_cap(size_t(optin))) {
+        cudaGetLastError();
+        return fail(CMC_ECUDA, "cudaFuncSetAttribute on the engine kernels failed");
+    }
     Ctx* planner = new (g_planner_storage[device]) Ctx();  // never destroyed: lives with the scratch
     planner->sms = sms;
     planner->smem_optin = size_t(optin);
@@ -196,8 +201,7 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
     const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
                    : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
                                      : (const void*)cmc_engine<uint32_t, uint32_t, true>;
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pl.smem_bytes));
-    if (e != cudaSuccess) return fail(CMC_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    // the engine's shared-memory limit was raised to the device maximum at set-up
     void* args[] = {&a};
     e = cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, s);
     if (e != cudaSuccess) return fail(CMC_ECUDA, std::string("engine launch: ") + cudaGetErrorString(e));

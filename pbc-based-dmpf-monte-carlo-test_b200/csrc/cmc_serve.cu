@@ -695,9 +695,7 @@ struct Server {
         const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
                        : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
                                          : (const void*)cmc_engine<uint32_t, uint32_t, true>;
-        if ((rc = cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(pl.smem_bytes)), "engine attribute")))
-            return rc;
+        // the context raised the engine's shared-memory limit to the device maximum
         void* args[] = {&a};
         if ((rc = cuda(cudaEventRecord(b.e0, st), "event"))) return rc;
         if ((rc = cuda(cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, st),
@@ -1017,9 +1015,7 @@ struct Server {
         const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
                        : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
                                          : (const void*)cmc_engine<uint32_t, uint32_t, true>;
-        if ((rc = cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(pl.smem_bytes)), "engine attribute")))
-            return rc;
+        // the context raised the engine's shared-memory limit to the device maximum
         void* args[] = {&a};
         if ((rc = cuda(cudaEventRecord(r_e0, st), "event"))) return rc;
         if ((rc = cuda(cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, st),

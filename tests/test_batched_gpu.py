@@ -63,3 +63,24 @@ def test_plan_classes(ctx, cmc):
     for i, (p, s, b, first, count) in enumerate(jobs):
         assert per_job[i] == ctx.launch(p, cmc.batch_key(s, b), first, count), i
         assert failed[i] == len(per_job[i])
+
+
+def test_graph_capture_and_replay(ctx, cmc):
+    # the same call shape runs eagerly, is captured, then replayed; other keys
+    # (other seeds and offsets, same shapes and counts) replay the same graph
+    jobs = random_mix(cmc, 10, 9)
+    results, states = [], []
+    for rnd in range(4):
+        js = [(p, s + rnd, b, first, count) for (p, s, b, first, count) in jobs]
+        results.append((ctx.run_jobs(js), js))
+        states.append(ctx.last_plan.rsplit("graph=", 1)[-1])
+    assert states == ["eager", "captured", "replayed", "replayed"], states
+    for (failed, per_job), js in results:
+        for i, (p, s, b, first, count) in enumerate(js):
+            assert per_job[i] == ctx.launch(p, cmc.batch_key(s, b), first, count), i
+    ctx.set_option("graph", 0)
+    try:
+        assert ctx.run_jobs(results[-1][1]) == results[-1][0]
+        assert "graph=" not in ctx.last_plan
+    finally:
+        ctx.set_option("graph", 1)

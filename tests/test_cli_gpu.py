@@ -100,3 +100,30 @@ def test_cli_extensions_k_and_overrides(tmp_path, oracle):
     assert failures(out, bt=10) == want
     s = json.loads((out / "summary.json").read_text())
     assert s["K_COPIES"] == 4 and s["BUCKETS_NUM"] == 72 and s["MAX_KICK_TIMES"] == 40
+
+
+def test_cli_large_table_checkpoint_resume(tmp_path, golden):
+    # config 4's table (t=16384, N=2^28) under a tighter load (B=19500, kick
+    # 300, ~20% failures): a run stopped after 3 of 8 batches and resumed with
+    # two workers matches an uninterrupted run, and batch 2's first trials
+    # match the reference's own CPU run of the same shape
+    def cli(out, *extra):
+        cmd = [str(BENCH), "--mode", "bgh25", "--et", "14", "--bt", "11", "--pnum", "16384",
+               "--ell-i", "28", "--buckets", "19500", "--max-kicks", "300", "--seed", "4",
+               "--input-mode", "affine", "--stop-after", str(1 << 20), "--out", str(out)]
+        r = subprocess.run(cmd + list(extra), capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        return json.loads((out / "summary.json").read_text())
+
+    clean = cli(tmp_path / "clean", "--workers", "1")
+    assert clean["status"] == "complete" and clean["completed"] == 1 << 14
+    part = cli(tmp_path / "resumed", "--workers", "1", "--max-batches", "3")
+    assert part["status"] == "budget" and part["completed"] == 3 << 11
+    done = cli(tmp_path / "resumed", "--workers", "2")
+    assert done["status"] == "complete" and done["failed"] == clean["failed"]
+    want = failures(tmp_path / "clean", bt=11)
+    assert failures(tmp_path / "resumed", bt=11) == want and len(want) > 1000
+    ref = next(r for r in golden["reference_runs"] if r["name"] == "config4_stress")
+    assert ref["batch"] == 2 and ref["first"] == 0
+    got = [t - (2 << 11) for t in want if (2 << 11) <= t < (2 << 11) + ref["count"]]
+    assert got == ref["failures"]
