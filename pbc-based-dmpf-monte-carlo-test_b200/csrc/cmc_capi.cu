@@ -181,7 +181,8 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
         return fail(CMC_EINVAL, "round cache of %u bytes does not fit shared memory", cache_bytes);
     // Slots.  A CTA walks about slots / (probes per trial x probe latency)
     // trials per cycle: ~2.4 t probes per trial, ~300 cycles per probe in
-    // shared memory, ~3000 in global memory (two dependent DRAM round trips
+    // shared memory (~800 when the walker shares its sub-partition with
+    // producers), ~3000 in global memory (two dependent DRAM round trips
     // once the slots outgrow L2).  Its producers build AES blocks at a
     // measured ~0.157 per cycle (direct passes, shared-memory cache) or ~0.2
     // (global round cache), over the job's blocks per trial.  Shared-memory
@@ -216,7 +217,9 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
         const uint32_t nw_g = (pl.isolate && !force_walkers) ? 4 : pl.nw;
         const uint32_t ng_g = groups_for(nw_g);
         const uint32_t ns_g = std::max<uint32_t>(1, std::min(kMaxSlots, 32 * nw_g) / ng_g) * ng_g;
-        const double walk_smem = pl.slots_smem ? pl.ns / (probes * 300.0) : 0.0;
+        // a walker beside ALU-bound producers issues slower: ~800 cycles per
+        // shared probe (measured at t=500, k=4), ~300 when isolated
+        const double walk_smem = pl.slots_smem ? pl.ns / (probes * (pl.isolate ? 300.0 : 800.0)) : 0.0;
         const double walk_global = ns_g / (probes * 3000.0);
         const bool keep_smem = pl.slots_smem && (!may_allocate || walk_smem >= 1.4 * produce ||
                                                  walk_smem >= walk_global);
@@ -331,6 +334,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
         a.group_off = pl.group_off;
         a.slots_off = pl.slots_off;
         a.spin_limit = spin_limit;
+        a.map_chains = map_chains;
         const void* fn =
             pl.walker_ctas
                 ? (pl.variant == 0   ? (const void*)cmc_engine_split<uint16_t, uint16_t, false>
@@ -562,10 +566,10 @@ std::string Ctx::graph_key(const std::vector<Job>& jobs, const std::vector<uint3
         key += b;
     }
     for (uint32_t x : bounds) key += std::to_string(x) + ",";
-    snprintf(b, sizeof b, "|%llu|%llu|%u/%u/%u/%u/%u/%d/%d/%d/%u|%p/%p/%p/%p/%p/%p/%p/%p",
+    snprintf(b, sizeof b, "|%llu|%llu|%u/%u/%u/%u/%u/%d/%d/%d/%u/%u|%p/%p/%p/%p/%p/%p/%p/%p",
              (unsigned long long)total, (unsigned long long)dev_cap, force_wg, force_ng,
              force_global_slots, force_walkers, max_slots_per_group, force_walker_ctas, force_isolate,
-             force_method, spin_limit, (void*)d_jobs, (void*)d_bits, (void*)d_out, (void*)d_slots,
+             force_method, spin_limit, map_chains, (void*)d_jobs, (void*)d_bits, (void*)d_out, (void*)d_slots,
              (void*)d_ctrl, (void*)d_job_failed, (void*)h_failed, (void*)h_nf);
     return key + b;
 }
@@ -925,6 +929,8 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
     else if (n == "method" && value >= -1 && value <= 2) c->force_method = int(value);
     else if (n == "graph" && (value == 0 || value == 1)) c->use_graphs = int(value);
+    else if (n == "map_chains" && (value == 0 || value == 1 || value == 2 || value == 4))
+        c->map_chains = uint32_t(value);
     else if (n == "walkers" && value >= 0 && value <= 4) c->force_walkers = uint32_t(value);
     else if (n == "isolate_walkers" && value >= -1 && value <= 1) c->force_isolate = int(value);
     else if (n == "walker_ctas" && value >= -1 && value < c->sms) c->force_walker_ctas = int(value);

@@ -93,6 +93,7 @@ struct Ctx {
     int force_method = -1;  // -1 auto, 0 direct, 1 cache (shared if h <= 12, else global), 2 global cache
     bool may_allocate = true;  // false: no global round cache, global slots only if unavoidable
     uint32_t spin_limit = 1u << 26;
+    uint32_t map_chains = 0;  // lookup chains per lane from a round cache (0: automatic)
 
     ~Ctx();
     int init(int dev);

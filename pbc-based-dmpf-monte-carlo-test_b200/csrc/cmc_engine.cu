@@ -270,6 +270,14 @@ __device__ __forceinline__ void build_map_cache(const Job& J, GroupHeader* gh,
     }
 }
 
+template <typename MapT>
+__device__ __forceinline__ void map_from_cache(const Job& J, GroupHeader* gh, const uint16_t* cache,
+                                               MapT* map, uint32_t lane, uint32_t chains) {
+    if (chains >= 4) build_map_cache<MapT, 4>(J, gh, cache, map, lane);
+    else if (chains == 2) build_map_cache<MapT, 2>(J, gh, cache, map, lane);
+    else build_map_cache<MapT, 1>(J, gh, cache, map, lane);
+}
+
 // Round cache: entry (r, R) = F_r(R) & mask for the 8 rounds and every h-bit
 // R, 8 * 2^h AES blocks.  Two independent blocks per iteration: their unrolled
 // round chains interleave, doubling the ILP of each warp.
@@ -474,13 +482,17 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
             sizeof(GroupHeader) + 2 * cache_entries <= a.group_bytes) {
             fill_round_cache(L, key, gh, cache, J.half_bits, (uint32_t)J.mask, gt, gthreads);
             group_sync(g, gthreads);
-            build_map_cache<MapT, 1>(J, gh, cache, map, lane);
+            map_from_cache<MapT>(J, gh, cache, map, lane, a.map_chains ? a.map_chains : 1);
         } else if (!WIDE && J.method == kMethodGCache && a.gcache != nullptr &&
                    cache_entries <= a.gcache_stride) {
             uint16_t* gc = a.gcache + (size_t)(blockIdx.x * a.ng + g) * a.gcache_stride;
             fill_round_cache(L, key, gh, gc, J.half_bits, (uint32_t)J.mask, gt, gthreads);
             group_sync(g, gthreads);  // orders the group's global writes before its reads
-            build_map_cache<MapT, 2>(J, gh, gc, map, lane);
+            // four chains hide L2/DRAM latency unless cycle-walking is heavy
+            // (c = 2^2h / D > 2), where idle chains' gathers cost more than
+            // the overlap gains (measured: t=1500, k=4, c~4: 4 chains 8% slower)
+            const bool light_walk = (1ULL << (2 * J.half_bits)) <= 2 * J.domain;
+            map_from_cache<MapT>(J, gh, gc, map, lane, a.map_chains ? a.map_chains : (light_walk ? 4 : 2));
         } else {
             build_map_direct<MapT, WIDE>(L, J, gh, key, map, lane);
         }

@@ -103,6 +103,7 @@ struct EngineArgs {
     // ring); entry_done[e] counts the finished walks of ring entry e
     const ResidentQueue* rq;
     uint32_t ring_mask;
+    uint32_t map_chains;                // lookup chains per lane from a round cache (0: automatic)
     unsigned long long entry_begin;
     unsigned long long bits_mask;
     unsigned int* entry_done;

@@ -692,6 +692,7 @@ struct Server {
         a.group_off = pl.group_off;
         a.slots_off = pl.slots_off;
         a.spin_limit = ctx->spin_limit;
+        a.map_chains = ctx->map_chains;
         const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
                        : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
                                          : (const void*)cmc_engine<uint32_t, uint32_t, true>;
@@ -1012,6 +1013,7 @@ struct Server {
         a.group_off = pl.group_off;
         a.slots_off = pl.slots_off;
         a.spin_limit = ctx->spin_limit;
+        a.map_chains = ctx->map_chains;
         const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
                        : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
                                          : (const void*)cmc_engine<uint32_t, uint32_t, true>;

@@ -21,11 +21,14 @@ ENGINE_VARIANTS = [
     {"isolate_walkers": 1, "warps_per_group": 1, "global_slots": 1},
     {"method": 2},                             # round cache in global memory (h <= 16)
     {"method": 2, "isolate_walkers": 1, "global_slots": 1, "warps_per_group": 4},
+    {"method": 1, "map_chains": 2},            # two lookup chains per lane (shared cache)
+    {"method": 2, "map_chains": 1},
+    {"method": 2, "map_chains": 4},
 ]
 
 
 DEFAULTS = {"method": -1, "global_slots": 0, "warps_per_group": 0, "groups": 0, "walkers": 0,
-            "walker_ctas": -1, "isolate_walkers": -1}
+            "walker_ctas": -1, "isolate_walkers": -1, "map_chains": 0}
 
 
 def apply(ctx, opts):
@@ -83,7 +86,7 @@ def reference_cases(golden):
     return [r["name"] for r in golden["reference_runs"]]
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 6, 7, 9, 10, 11, 12])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 6, 7, 9, 10, 11, 12, 13, 14, 15])
 def test_reference_runs(ctx, cmc, golden, variant):
     apply(ctx, ENGINE_VARIANTS[variant])
     for r in golden["reference_runs"]:
@@ -112,7 +115,7 @@ def random_shapes(n, seed):
 @pytest.mark.parametrize("shape", random_shapes(24, 7))
 def test_vs_oracle_random_shapes(ctx, cmc, oracle, shape):
     mode, im, pnum, ell, k, buckets, kick, seed, batch = shape
-    apply(ctx, ENGINE_VARIANTS[[0, 6, 7, 9, 10, 11, 12][seed % 7]])
+    apply(ctx, ENGINE_VARIANTS[[0, 6, 7, 9, 10, 11, 12, 13, 15][seed % 9]])
     p = cmc.parameters(mode, pnum, ell, k, buckets, kick, im)
     op = oracle.params(mode, pnum, ell, k, buckets, kick, im)
     count = 512 if pnum <= 100 else 96
