@@ -137,14 +137,19 @@ int cmc_server_create(cmc_ctx* ctx, uint32_t max_jobs, uint64_t mem_budget_bytes
                       uint32_t batch_bits, uint64_t max_iteration_trials, cmc_server** out);
 int cmc_server_submit(cmc_server* server, const cmc_params* params, uint64_t seed,
                       uint64_t trials, const char* journal_dir, uint32_t* out_id);
-/* One iteration; work_blocks is its minimum AES-block budget (it grows to an
- * eighth of the outstanding work of the granted size class, at most 20x, and
- * to 2.5x the latency of the slowest trial granted).  Iterations are
- * pipelined two deep: a call issues its iteration on one of two streams and
- * then commits the previous call's iteration, which ran meanwhile, so a job
- * is reported finished (up to cap ids in out_finished) by the call after the
- * one that issued its last trials.  cmc_server_destroy commits the
- * iterations still in flight before it frees the server. */
+/* One step.  Resident serving (the default): reads back finished work,
+ * admits queued jobs, publishes grants worth about work_blocks AES blocks
+ * whenever less than twice that is still unclaimed by the running launch,
+ * and starts a launch if none runs; jobs are reported finished (up to cap ids
+ * in out_finished) by the step that reads back their last trials.
+ * Iterations ("resident" 0): work_blocks is the minimum AES-block budget of
+ * the step's engine launch (it grows to an eighth of the outstanding work of
+ * the granted size class, at most 20x, and to 2.5x the latency of the
+ * slowest trial granted); launches are pipelined two deep, so a job is
+ * reported by the call after the one that issued its last trials.
+ * cmc_server_destroy commits the work still in flight before it frees the
+ * server.  After a step returns an error (a device wait that gave up, a CUDA
+ * error) the server's state is undefined: destroy it. */
 int cmc_server_step(cmc_server* server, uint64_t work_blocks, uint32_t* out_finished,
                     uint32_t cap, uint32_t* out_nfinished);
 /* out_state: 0 queued, 1 running, 2 done. */
@@ -191,8 +196,9 @@ int cmc_server_destroy(cmc_server* server);
  * on SM sub-partition 3, producers on 0..2), "slots_per_group" (cap on
  * shared-memory slots per group, default 8), "walker_ctas" (-1 auto, 0 walks
  * inside each CTA, N > 0 dedicates N CTAs -- one per SM -- to walks over
- * global slots while the others only build maps), "spin_limit" (polls before
- * a device wait gives up), "graph" (1, the default: cmc_run_jobs captures the
+ * global slots while the others only build maps), "spin_limit" (microseconds
+ * a device wait may last before it gives up with CMC_ETIMEOUT; default 2^26,
+ * about 67 s), "graph" (1, the default: cmc_run_jobs captures the
  * device side of a call shape -- job shapes, counts and buffers -- into a CUDA
  * graph on its second call and replays it from the third; 0: always eager),
  * "map_chains" (0 automatic, or 1, 2, 4: candidate lookup chains per lane

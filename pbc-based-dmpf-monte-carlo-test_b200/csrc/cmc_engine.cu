@@ -17,8 +17,9 @@
 // compacted in order by cmc_compact_failures (the reference appends offsets
 // through an atomic counter and sorts on the host, cuckoo_bench.cu:313-316,738).
 //
-// All waits (slot hand-off, end of work) are bounded: after spin_limit polls
-// the kernel records CMC_ETIMEOUT in Ctrl and returns.
+// All waits (slot hand-off, end of work, new work in a resident launch) are
+// bounded in time: after spin_limit microseconds (%globaltimer) the kernel
+// records CMC_ETIMEOUT in Ctrl, with the waiting site in `where`, and returns.
 #include <cstdint>
 
 #include "cmc_aes.cuh"
@@ -352,7 +353,7 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
                     nap = min(nap * 2, 131072u);
                     if (globaltimer_ns() - t_start > 1000ULL * a.spin_limit) {
                         atomicExch(&a.ctrl->error, kErrTimeout);
-                        atomicExch(&a.ctrl->where, 4u);
+                        atomicExch(&a.ctrl->where, 6u);
                         break;
                     }
                 }
@@ -418,8 +419,9 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
             // Claim a free slot (FREE -> FILLING).  In-CTA slots: any free
             // one, starting from this group's share of the pool.  Split
             // engine: the next slot of a global ring, waiting for its walk.
-            uint32_t spins = 0, slot = 0xffffffffu;
+            uint32_t slot = 0xffffffffu;
             const long long wait0 = clock64();
+            const unsigned long long wait_ns = globaltimer_ns();
             uint32_t ring = 0;
             if constexpr (SPLIT) ring = atomicAdd(&a.ctrl->slot_cursor, 1u) % a.ns;
             for (;;) {
@@ -436,7 +438,7 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
                 }
                 if (slot != 0xffffffffu) break;
                 __nanosleep(128);
-                if (++spins > a.spin_limit) {
+                if (globaltimer_ns() - wait_ns > 1000ULL * a.spin_limit) {
                     atomicExch(&a.ctrl->error, kErrTimeout);
                     atomicExch(&a.ctrl->where, 1u);
                     gh->abort = 1;
@@ -740,7 +742,7 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
     unsigned long long gidx = 0;
     uint32_t job = 0;
     unsigned long long probes = 0, walks = 0, idle_cycles = 0;
-    uint32_t idle = 0;
+    unsigned long long idle_since = 0;  // start of the current idle stretch (ns)
     const long long born = clock64();
     for (;;) {
         if (!busy && owner && ld_acquire(&cs->slot_state[my]) == kSlotReady) {
@@ -781,9 +783,10 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
             if (!__any_sync(kFull, ready)) {
                 if (done) break;
                 const long long t0 = clock64();
+                if (!idle_since) idle_since = globaltimer_ns();
                 __nanosleep(128);
                 idle_cycles += (unsigned long long)(clock64() - t0);
-                if (++idle > a.spin_limit) {
+                if (globaltimer_ns() - idle_since > 1000ULL * a.spin_limit) {
                     if (lane == 0) {
                         atomicExch(&a.ctrl->error, kErrTimeout);
                         atomicExch(&a.ctrl->where, 2u);
@@ -792,7 +795,7 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
                 }
             }
         } else {
-            idle = 0;
+            idle_since = 0;
         }
     }
     // warp totals for diagnostics
@@ -822,7 +825,7 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
     unsigned long long gidx = 0;
     uint32_t job = 0;
     unsigned long long probes = 0, walks = 0, idle_cycles = 0;
-    uint32_t idle = 0;
+    unsigned long long idle_since = 0;  // start of the current idle stretch (ns)
     const long long born = clock64();
     for (;;) {
         if (!busy && owner && ld_acquire_gpu(&hdr->state) == kSlotReady) {
@@ -866,9 +869,10 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
             if (!__any_sync(kFull, ready)) {
                 if (done) break;
                 const long long t0 = clock64();
+                if (!idle_since) idle_since = globaltimer_ns();
                 __nanosleep(256);
                 idle_cycles += (unsigned long long)(clock64() - t0);
-                if (++idle > a.spin_limit) {
+                if (globaltimer_ns() - idle_since > 1000ULL * a.spin_limit) {
                     if (lane == 0) {
                         atomicExch(&a.ctrl->error, kErrTimeout);
                         atomicExch(&a.ctrl->where, 4u);
@@ -877,7 +881,7 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
                 }
             }
         } else {
-            idle = 0;
+            idle_since = 0;
         }
     }
     for (int o = 16; o; o >>= 1) {

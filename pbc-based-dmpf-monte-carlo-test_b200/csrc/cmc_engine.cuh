@@ -91,7 +91,7 @@ struct EngineArgs {
     uint32_t group_bytes;               // per-group smem (header + cache)
     uint32_t group_off;                 // smem offset of group 0
     uint32_t slots_off;                 // smem offset of slot 0 (smem slots)
-    uint32_t spin_limit;                // bounded waits (polls of ~0.5 us)
+    uint32_t spin_limit;                // bounded waits: microseconds before one gives up
     // global round caches (kMethodGCache jobs): group (cta, g) owns entries
     // [(cta * ng + g) * gcache_stride, +8 << h)
     uint16_t* gcache;
