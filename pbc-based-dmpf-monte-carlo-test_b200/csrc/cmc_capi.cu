@@ -264,6 +264,9 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
              uint32_t* d_out, uint32_t* d_count, uint64_t out_cap_now,
              unsigned long long* job_failed, unsigned long long* job_done,
              const std::vector<uint32_t>* bounds_in) {
+    // launch checks below read cudaGetLastError: start from a clean slate (an
+    // earlier non-fatal error, e.g. of a timing query, is not this launch's)
+    cudaGetLastError();
     std::vector<uint32_t> bounds = bounds_in ? *bounds_in : std::vector<uint32_t>{0, uint32_t(jobs.size())};
     const uint32_t nclass = uint32_t(bounds.size()) - 1;
     if (nclass < 1 || nclass > kMaxClasses) return fail(CMC_EINVAL, "bad plan classes");
@@ -295,7 +298,9 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     if (pool && (rc = grow(d_slots, slots_cap, size_t(pool), "slot and cache pool"))) return rc;
     if ((rc = cuda(cudaMemsetAsync(d_ctrl, 0, nclass * sizeof(Ctrl), st), "memset ctrl"))) return rc;
     if ((rc = cuda(cudaMemsetAsync(d_bits, 0, words * 4, st), "memset bitmap"))) return rc;
-    if ((rc = cuda(cudaEventRecord(ev_start, st), "event"))) return rc;
+    // timing events stay out of captured graphs: a replay records them
+    // around the graph launch instead
+    if (!capturing && (rc = cuda(cudaEventRecord(ev_start, st), "event"))) return rc;
     kernels = 0;
     for (uint32_t c = 0; c < nclass; ++c) {
         const Plan& pl = plans[c];
@@ -354,7 +359,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
             return rc;
         ++kernels;
     }
-    if ((rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
+    if (!capturing && (rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
     if (d_out) {
         cmc_compact_failures<<<1, 1024, 0, st>>>(d_bits, total, value_base, d_out, d_count, out_cap_now,
                                                  nullptr);
@@ -717,7 +722,9 @@ int Ctx::run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t*
         const std::string key = graph_key(jobs, bounds, total, dev_cap);
         auto it = std::find_if(graphs.begin(), graphs.end(), [&](const GraphEntry& g) { return g.key == key; });
         if (it != graphs.end()) {
+            if ((rc = cuda(cudaEventRecord(ev_start, st), "event"))) return rc;
             if ((rc = cuda(cudaGraphLaunch(it->exec, st), "graph launch"))) return rc;
+            if ((rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
             kernels = it->kernels;
             ctrl_count = it->ctrl_count;
             plan_text = it->plan_text;
@@ -740,7 +747,9 @@ int Ctx::run_jobs(const cmc_job* in, uint32_t n, uint64_t* out_failed, uint32_t*
                 }
                 graphs.push_back(GraphEntry{key, ex, kernels, ctrl_count, plan_text, last_plan});
                 if (g) cudaGraphDestroy(g);
+                if ((rc = cuda(cudaEventRecord(ev_start, st), "event"))) return rc;
                 if ((rc = cuda(cudaGraphLaunch(ex, st), "graph launch"))) return rc;
+                if ((rc = cuda(cudaEventRecord(ev_stop, st), "event"))) return rc;
                 graph_state = "captured";
             } else {
                 // the shape could not be captured: run it eagerly
@@ -953,8 +962,12 @@ double cmc_last_engine_ms(cmc_ctx* ctx) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     if (c->kernels == 0) return -1.0;
     float ms = 0.f;
-    if (cudaEventSynchronize(c->ev_stop) != cudaSuccess) return -1.0;
-    if (cudaEventElapsedTime(&ms, c->ev_start, c->ev_stop) != cudaSuccess) return -1.0;
+    // a failure here must not stay pending for the next launch's error check
+    if (cudaEventSynchronize(c->ev_stop) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, c->ev_start, c->ev_stop) != cudaSuccess) {
+        cudaGetLastError();
+        return -1.0;
+    }
     return ms;
 }
 

@@ -655,6 +655,7 @@ struct Server {
             return rc;
         // schedulers run in issue order: each advances the RNG counters the
         // next one starts from
+        cudaGetLastError();  // launch checks below read it: drop earlier non-fatal errors
         const StepBuf& other = bufs[(&b == &bufs[0]) ? 1 : 0];
         if (sched_seen && (rc = cuda(cudaStreamWaitEvent(st, other.sched_done, 0), "order schedulers")))
             return rc;
@@ -1188,6 +1189,8 @@ struct Server {
                 if ((rc = resident_finished())) return rc;
             } else if (q != cudaErrorNotReady) {
                 return cuda(q, "resident launch");
+            } else {
+                cudaGetLastError();  // "not ready" is an answer, not an error to keep
             }
         }
         uint32_t consumed = 0;

@@ -74,6 +74,7 @@ def test_graph_capture_and_replay(ctx, cmc):
         js = [(p, s + rnd, b, first, count) for (p, s, b, first, count) in jobs]
         results.append((ctx.run_jobs(js), js))
         states.append(ctx.last_plan.rsplit("graph=", 1)[-1])
+        assert ctx.last_engine_ms() > 0     # timing works across capture and replay
     assert states == ["eager", "captured", "replayed", "replayed"], states
     for (failed, per_job), js in results:
         for i, (p, s, b, first, count) in enumerate(js):
