@@ -196,10 +196,11 @@ int cmc_server_destroy(cmc_server* server);
  * on SM sub-partition 3, producers on 0..2), "slots_per_group" (cap on
  * shared-memory slots per group, default 8), "walker_ctas" (-1 auto, 0 walks
  * inside each CTA, N > 0 dedicates N CTAs -- one per SM -- to walks over
- * global slots while the others only build maps), "spin_limit" (microseconds
- * a device wait may last before it gives up with CMC_ETIMEOUT; default 2^26,
- * about 67 s), "graph" (1, the default: cmc_run_jobs captures the
- * device side of a call shape -- job shapes, counts and buffers -- into a CUDA
+ * global slots while the others only build maps), "spin_limit" (bound of a
+ * device wait before it gives up with CMC_ETIMEOUT: microseconds for producer
+ * waits, polls of a fraction of a microsecond for idle walkers -- 32x as many
+ * in a resident server launch; default 2^26, about 67 s for producers),
+ * "graph" (1, the default: cmc_run_jobs captures the device side of a call shape -- job shapes, counts and buffers -- into a CUDA
  * graph on its second call and replays it from the third; 0: always eager),
  * "map_chains" (0 automatic, or 1, 2, 4: candidate lookup chains per lane
  * when a bucket map is built from a round cache).

@@ -339,6 +339,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
         a.group_off = pl.group_off;
         a.slots_off = pl.slots_off;
         a.spin_limit = spin_limit;
+        a.idle_polls = spin_limit;
         a.map_chains = map_chains;
         const void* fn =
             pl.walker_ctas

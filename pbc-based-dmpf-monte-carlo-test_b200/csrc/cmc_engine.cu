@@ -17,9 +17,13 @@
 // compacted in order by cmc_compact_failures (the reference appends offsets
 // through an atomic counter and sorts on the host, cuckoo_bench.cu:313-316,738).
 //
-// All waits (slot hand-off, end of work, new work in a resident launch) are
-// bounded in time: after spin_limit microseconds (%globaltimer) the kernel
-// records CMC_ETIMEOUT in Ctrl, with the waiting site in `where`, and returns.
+// All waits are bounded.  Producer waits (a free slot, new work in a resident
+// launch) give up after spin_limit microseconds (%globaltimer); idle walkers
+// count polls instead (a timer read in their loop measured 5x slower walks on
+// global slots, as did one more value held across their loop) and give up
+// after idle_polls polls, which the host always sets.  The
+// kernel then records CMC_ETIMEOUT in Ctrl, with the waiting site in `where`,
+// and returns.
 #include <cstdint>
 
 #include "cmc_aes.cuh"
@@ -742,7 +746,7 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
     unsigned long long gidx = 0;
     uint32_t job = 0;
     unsigned long long probes = 0, walks = 0, idle_cycles = 0;
-    unsigned long long idle_since = 0;  // start of the current idle stretch (ns)
+    uint32_t idle = 0;
     const long long born = clock64();
     for (;;) {
         if (!busy && owner && ld_acquire(&cs->slot_state[my]) == kSlotReady) {
@@ -783,10 +787,9 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
             if (!__any_sync(kFull, ready)) {
                 if (done) break;
                 const long long t0 = clock64();
-                if (!idle_since) idle_since = globaltimer_ns();
                 __nanosleep(128);
                 idle_cycles += (unsigned long long)(clock64() - t0);
-                if (globaltimer_ns() - idle_since > 1000ULL * a.spin_limit) {
+                if (++idle > a.idle_polls) {  // a kernel parameter: no register held in the loop
                     if (lane == 0) {
                         atomicExch(&a.ctrl->error, kErrTimeout);
                         atomicExch(&a.ctrl->where, 2u);
@@ -795,7 +798,7 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
                 }
             }
         } else {
-            idle_since = 0;
+            idle = 0;
         }
     }
     // warp totals for diagnostics
@@ -825,7 +828,7 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
     unsigned long long gidx = 0;
     uint32_t job = 0;
     unsigned long long probes = 0, walks = 0, idle_cycles = 0;
-    unsigned long long idle_since = 0;  // start of the current idle stretch (ns)
+    uint32_t idle = 0;
     const long long born = clock64();
     for (;;) {
         if (!busy && owner && ld_acquire_gpu(&hdr->state) == kSlotReady) {
@@ -869,10 +872,9 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
             if (!__any_sync(kFull, ready)) {
                 if (done) break;
                 const long long t0 = clock64();
-                if (!idle_since) idle_since = globaltimer_ns();
                 __nanosleep(256);
                 idle_cycles += (unsigned long long)(clock64() - t0);
-                if (globaltimer_ns() - idle_since > 1000ULL * a.spin_limit) {
+                if (++idle > a.idle_polls) {  // a kernel parameter: no register held in the loop
                     if (lane == 0) {
                         atomicExch(&a.ctrl->error, kErrTimeout);
                         atomicExch(&a.ctrl->where, 4u);
@@ -881,7 +883,7 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
                 }
             }
         } else {
-            idle_since = 0;
+            idle = 0;
         }
     }
     for (int o = 16; o; o >>= 1) {

@@ -91,7 +91,8 @@ struct EngineArgs {
     uint32_t group_bytes;               // per-group smem (header + cache)
     uint32_t group_off;                 // smem offset of group 0
     uint32_t slots_off;                 // smem offset of slot 0 (smem slots)
-    uint32_t spin_limit;                // bounded waits: microseconds before one gives up
+    uint32_t spin_limit;                // producer waits: microseconds before one gives up
+    uint32_t idle_polls;                // idle-walker polls before giving up (set by every launch)
     // global round caches (kMethodGCache jobs): group (cta, g) owns entries
     // [(cta * ng + g) * gcache_stride, +8 << h)
     uint16_t* gcache;

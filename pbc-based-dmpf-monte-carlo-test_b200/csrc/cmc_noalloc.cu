@@ -198,6 +198,7 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
     a.group_off = pl.group_off;
     a.slots_off = pl.slots_off;
     a.spin_limit = pl_ctx.spin_limit;
+    a.idle_polls = pl_ctx.spin_limit;
     const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
                    : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
                                      : (const void*)cmc_engine<uint32_t, uint32_t, true>;

@@ -693,6 +693,7 @@ struct Server {
         a.group_off = pl.group_off;
         a.slots_off = pl.slots_off;
         a.spin_limit = ctx->spin_limit;
+        a.idle_polls = ctx->spin_limit;
         a.map_chains = ctx->map_chains;
         const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
                        : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
@@ -998,6 +999,9 @@ struct Server {
         a.ring_mask = kRing - 1;
         a.entry_begin = e_begin;
         a.entry_done = d_rdone;
+        // walkers idle while producers wait on the host for new work: give
+        // them a bound in polls well past the producers' bound in time
+        a.idle_polls = uint32_t(std::min<uint64_t>(0xffffffffULL, 32ULL * ctx->spin_limit));
         a.gslots = pl.slots_smem ? nullptr : d_rpool;
         a.gcache = pl.gcache_bytes ? reinterpret_cast<uint16_t*>(d_rpool + cache_offset(pl)) : nullptr;
         a.gcache_stride = pl.gcache_stride;
