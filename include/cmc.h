@@ -202,7 +202,7 @@ int cmc_server_destroy(cmc_server* server);
  * in a resident server launch; default 2^26, about 67 s for producers),
  * "graph" (1, the default: cmc_run_jobs captures the device side of a call shape -- job shapes, counts and buffers -- into a CUDA
  * graph on its second call and replays it from the third; 0: always eager),
- * "map_chains" (0 automatic, or 1, 2, 4: candidate lookup chains per lane
+ * "map_chains" (0 automatic, or 1, 2, 4, 8: candidate lookup chains per lane
  * when a bucket map is built from a round cache).
  * Returns CMC_EINVAL for an unknown name or a value out of range. */
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);

@@ -939,7 +939,7 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
     else if (n == "method" && value >= -1 && value <= 2) c->force_method = int(value);
     else if (n == "graph" && (value == 0 || value == 1)) c->use_graphs = int(value);
-    else if (n == "map_chains" && (value == 0 || value == 1 || value == 2 || value == 4))
+    else if (n == "map_chains" && (value == 0 || value == 1 || value == 2 || value == 4 || value == 8))
         c->map_chains = uint32_t(value);
     else if (n == "walkers" && value >= 0 && value <= 4) c->force_walkers = uint32_t(value);
     else if (n == "isolate_walkers" && value >= -1 && value <= 1) c->force_isolate = int(value);

@@ -278,7 +278,8 @@ __device__ __forceinline__ void build_map_cache(const Job& J, GroupHeader* gh,
 template <typename MapT>
 __device__ __forceinline__ void map_from_cache(const Job& J, GroupHeader* gh, const uint16_t* cache,
                                                MapT* map, uint32_t lane, uint32_t chains) {
-    if (chains >= 4) build_map_cache<MapT, 4>(J, gh, cache, map, lane);
+    if (chains >= 8) build_map_cache<MapT, 8>(J, gh, cache, map, lane);
+    else if (chains >= 4) build_map_cache<MapT, 4>(J, gh, cache, map, lane);
     else if (chains == 2) build_map_cache<MapT, 2>(J, gh, cache, map, lane);
     else build_map_cache<MapT, 1>(J, gh, cache, map, lane);
 }
