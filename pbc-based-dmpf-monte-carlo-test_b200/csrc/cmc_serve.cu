@@ -366,11 +366,23 @@ struct Server {
 
     static uint64_t cache_offset(const Plan& pl) { return (pl.gslot_bytes + 255) / 256 * 256; }
 
-    std::vector<uint32_t> active_ids() const {
-        std::vector<uint32_t> v;
-        for (const HostJob& j : jobs)
-            if (j.state == 1) v.push_back(j.id);
-        return v;
+    // Admitted, unfinished jobs in admission order, and the number of jobs not
+    // finished yet: kept up to date so that a long-lived server's steps do not
+    // scan every job it has ever seen.
+    std::vector<uint32_t> active_list;
+    uint32_t unfinished = 0;
+
+    std::vector<uint32_t> active_ids() const { return active_list; }
+
+    void activate(HostJob& j) {
+        j.state = 1;
+        active_list.push_back(j.id);
+    }
+
+    void finish(HostJob& j) {
+        if (j.state == 1) active_list.erase(std::find(active_list.begin(), active_list.end(), j.id));
+        j.state = 2;
+        --unfinished;
     }
 
     int submit(const cmc_params& p, uint64_t seed, uint64_t trials, const char* journal_dir,
@@ -435,6 +447,7 @@ struct Server {
         }
         jobs.push_back(std::move(j));
         queue.push_back(jobs.back().id);
+        ++unfinished;
         if (out_id) *out_id = jobs.back().id;
         return CMC_OK;
     }
@@ -448,7 +461,7 @@ struct Server {
             HostJob& j = jobs[id];
             if (j.next >= j.budget) {  // fully journaled already
                 queue.pop_front();
-                j.state = 2;
+                finish(j);
                 continue;
             }
             std::vector<uint32_t> ids = active_ids();
@@ -467,7 +480,7 @@ struct Server {
             queue.pop_front();
             j.slot = free_slots.back();
             free_slots.pop_back();
-            j.state = 1;
+            activate(j);
             j.admitted_at = iteration;
             ServeState state{};
             rc = ctx->make_job(j.params, 0, 1, 0, state.job);
@@ -792,7 +805,7 @@ struct Server {
                 j.pending.erase(j.pending.begin());
             }
             if (j.state == 1 && j.processed >= j.budget && j.pending.empty()) {
-                j.state = 2;
+                finish(j);
                 j.journal.reset();
                 free_slots.push_back(j.slot);
                 if (finished && nfin < cap) finished[nfin] = id;
@@ -1174,7 +1187,7 @@ struct Server {
                 j.pending.erase(j.pending.begin());
             }
             if (j.processed >= j.budget && j.pending.empty()) {
-                j.state = 2;
+                finish(j);
                 j.journal.reset();
                 free_slots.push_back(j.slot);
                 if (finished && nfin < cap) finished[nfin] = id;
@@ -1316,10 +1329,7 @@ int cmc_server_get_stats(const cmc_server* server, cmc_server_stats* out) {
 
 uint32_t cmc_server_pending(const cmc_server* server) {
     if (!server) return 0;
-    const Server* s = reinterpret_cast<const Server*>(server);
-    uint32_t n = 0;
-    for (const auto& j : s->jobs) n += j.state != 2;
-    return n;
+    return reinterpret_cast<const Server*>(server)->unfinished;
 }
 
 const char* cmc_server_error(const cmc_server* server) {
