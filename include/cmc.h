@@ -244,6 +244,13 @@ int cmc_last_stats(cmc_ctx* ctx, uint64_t out[6]);
 uint32_t cmc_last_kernel_count(const cmc_ctx* ctx);
 /* Human-readable description of the last launch plan (engine, groups, ...). */
 const char* cmc_last_plan(const cmc_ctx* ctx);
+/* No counterpart in the reference.  Planner dry run, no device needed: writes
+ * to out (cap bytes) the plan text cmc_launch would report for count trials
+ * of params on a device with `sms` SMs and `smem_optin` bytes of opt-in
+ * shared memory per block (148 and 232448 on B200), with default options.
+ * Returns 0, or a CMC_E* code with the reason in out. */
+int cmc_plan_describe(const cmc_params* params, uint32_t count, uint32_t sms, uint64_t smem_optin,
+                      char* out, uint32_t cap);
 
 #ifdef __cplusplus
 }

@@ -35,7 +35,7 @@ CMC_ENOMEM = -6
 EXPORTS = (
     "cmc_derive_params", "cmc_batch_key", "cmc_host_aes128", "cmc_init", "cmc_destroy",
     "cmc_last_error", "cmc_launch", "cmc_launch_device", "cmc_check",
-    "cmc_last_kernel_count", "cmc_last_plan", "cmc_set_option",
+    "cmc_last_kernel_count", "cmc_last_plan", "cmc_plan_describe", "cmc_set_option",
     "cmc_set_stream", "cmc_last_engine_ms", "cmc_last_stats", "cmc_launch_static",
     "cmc_run_jobs", "cmc_autotune", "cmc_server_create", "cmc_server_submit", "cmc_server_step",
     "cmc_server_status", "cmc_server_pending", "cmc_server_error", "cmc_server_destroy",
@@ -153,6 +153,9 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     lib.cmc_server_destroy.restype = ctypes.c_int
     lib.cmc_last_plan.argtypes = [vp]
     lib.cmc_last_plan.restype = ctypes.c_char_p
+    lib.cmc_plan_describe.argtypes = [ctypes.POINTER(Params), u32, u32, ctypes.c_uint64,
+                                      ctypes.c_char_p, u32]
+    lib.cmc_plan_describe.restype = ctypes.c_int
     if path is None:
         _lib = lib
     return lib
@@ -168,6 +171,17 @@ def parameters(mode: str = "bgh25", pnum: int = 16, ell_i: int = 32, k: int = 3,
     if rc:
         raise CmcError(rc, "invalid parameters")
     return p
+
+
+def plan_describe(params: Params, count: int, sms: int = 148, smem_optin: int = 232448) -> str:
+    """Planner dry run without a device: the plan cmc_launch would choose for
+    `count` trials (defaults: B200's SM count and opt-in shared memory)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(512)
+    rc = lib.cmc_plan_describe(ctypes.byref(params), count, sms, smem_optin, buf, len(buf))
+    if rc:
+        raise CmcError(rc, buf.value.decode())
+    return buf.value.decode()
 
 
 def batch_key(seed: int, batch_id: int) -> list[int]:

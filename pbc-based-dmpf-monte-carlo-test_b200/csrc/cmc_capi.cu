@@ -459,7 +459,8 @@ int Ctx::init(int dev) {
 }
 
 Ctx::~Ctx() {
-    if (device >= 0) cudaSetDevice(device);
+    if (device < 0) return;  // a planner that never touched a device holds nothing to free
+    cudaSetDevice(device);
     cudaFree(d_t0);
     cudaFree(d_ctrl);
     cudaFree(d_jobs);
@@ -987,6 +988,25 @@ int cmc_last_stats(cmc_ctx* ctx, uint64_t out[6]) {
 
 uint32_t cmc_last_kernel_count(const cmc_ctx* ctx) {
     return ctx ? reinterpret_cast<const Ctx*>(ctx)->kernels : 0;
+}
+
+int cmc_plan_describe(const cmc_params* params, uint32_t count, uint32_t sms, uint64_t smem_optin,
+                      char* out, uint32_t cap) {
+    if (!params || !out || cap == 0 || count == 0 || sms == 0 ||
+        smem_optin < uint64_t(cmc::kEngineTableBytes) + cmc::kCtaSharedBytes + cmc::kGroupHeaderBytes) {
+        cmc::set_thread_error("cmc_plan_describe: invalid argument");
+        return CMC_EINVAL;
+    }
+    Ctx c;  // planner only: no device is selected and nothing is allocated
+    c.sms = int(sms);
+    c.smem_optin = size_t(smem_optin);
+    std::vector<cmc::Job> jobs(1);
+    int rc = c.make_job(*params, 0, count, 0, jobs[0]);
+    cmc::Plan pl;
+    if (!rc) rc = c.plan(jobs, pl);
+    snprintf(out, cap, "%s", (rc ? c.err : c.plan_text).c_str());
+    if (rc) cmc::set_thread_error(c.err);
+    return rc;
 }
 
 const char* cmc_last_plan(const cmc_ctx* ctx) {
