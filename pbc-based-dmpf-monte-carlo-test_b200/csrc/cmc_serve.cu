@@ -40,6 +40,7 @@
 #include "cmc_aes.cuh"
 #include "cmc_capi_internal.hpp"
 #include "cmc_engine.cuh"
+#include "cmc_grants.hpp"
 #include "cmc_hostcore.hpp"
 #include "cmc_runner.hpp"
 
@@ -570,69 +571,18 @@ struct Server {
         std::vector<uint32_t> ids;
         for (uint32_t id : all)
             if (!one_class || jobs[id].global_slots == cls) ids.push_back(id);
-        // grants: fifo_share of the work in arrival order (bounds the tail),
-        // the rest shortest remaining work first (small jobs finish at once);
-        // the step is at least 2.5x the latency of its slowest trial so that
-        // trial's tail is covered
-        std::vector<uint32_t> order = ids;
-        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return remaining(a) < remaining(b); });
-        double floor_blocks = 0;
-        for (uint32_t id : ids) floor_blocks = std::max(floor_blocks, 2.5 * jobs[id].latency_blocks);
-        // Backlog-adaptive size: an eighth of the class's outstanding work,
-        // between work_blocks and 20x work_blocks.  A light load runs short
-        // iterations (an arrival waits little); a backlog runs long ones
-        // (fewer iteration tails, measured 1.2x throughput at 20x).
-        double backlog = 0;
-        for (uint32_t id : ids) backlog += remaining(id);
-        const double adaptive = std::min(backlog / 8.0, 20.0 * double(work_blocks));
-        work_blocks = std::max<uint64_t>({work_blocks, uint64_t(floor_blocks), uint64_t(adaptive)});
-        // shares per job (trials), then one grant per job
-        std::vector<uint64_t> share(ids.size(), 0);
-        std::vector<uint32_t> pos(jobs.size(), 0);
-        for (uint32_t i = 0; i < ids.size(); ++i) pos[ids[i]] = i;
-        double left = double(work_blocks);
-        uint64_t trials_left = max_iter_trials;
-        auto room = [&](uint32_t id) {  // trials this job can still take in this step
+        // the policy itself (cmc_grants.hpp): work size, arrival-order and
+        // shortest-work shares, batch boundaries, heaviest-first order
+        std::vector<GrantCandidate> cands;
+        for (uint32_t id : ids) {
             const HostJob& j = jobs[id];
-            const uint64_t per = 1ULL << j.bt;
-            const uint64_t next = j.next + share[pos[id]];
-            uint64_t r = std::min<uint64_t>(j.budget - next, per - (next & (per - 1)));
-            if (share[pos[id]] > 0 && (next & (per - 1)) == 0) r = 0;  // one batch per grant
-            return std::min<uint64_t>(r, 0xffffffffULL - share[pos[id]]);
-        };
-        auto give = [&](uint32_t id, double blocks) {
-            const HostJob& j = jobs[id];
-            uint64_t n = uint64_t(std::max(1.0, blocks / j.cost));
-            n = std::min<uint64_t>({n, room(id), trials_left});
-            share[pos[id]] += n;
-            trials_left -= n;
-            left -= double(n) * j.cost;
-        };
-        std::vector<uint32_t> fifo = ids;
-        std::sort(fifo.begin(), fifo.end(), [&](uint32_t a, uint32_t b) {
-            return jobs[a].admitted_at != jobs[b].admitted_at ? jobs[a].admitted_at < jobs[b].admitted_at : a < b;
-        });
-        const double keep = double(work_blocks) * (1.0 - fifo_share);
-        for (uint32_t id : fifo) {
-            if (left <= keep || trials_left == 0) break;
-            give(id, left - keep);
+            cands.push_back(GrantCandidate{id, j.next, j.budget, j.bt, j.cost, j.latency_blocks, j.admitted_at});
         }
-        for (uint32_t id : order) {
-            if (left <= 0 || trials_left == 0) break;
-            give(id, left);
-        }
-        // the table runs heaviest trials first (as cmc_run_jobs does), so the
-        // iteration ends on short trials instead of on the longest walks
-        std::vector<uint32_t> heavy;
-        for (uint32_t i = 0; i < ids.size(); ++i)
-            if (share[i] > 0) heavy.push_back(i);
-        std::stable_sort(heavy.begin(), heavy.end(),
-                         [&](uint32_t a, uint32_t b) { return jobs[ids[a]].cost > jobs[ids[b]].cost; });
-        for (uint32_t i : heavy) {
-            HostJob& j = jobs[ids[i]];
-            grants.push_back(Grant{j.slot, uint32_t(share[i])});
-            grant_jobs.push_back(ids[i]);
-            j.next += share[i];
+        for (const GrantShare& g : grant_shares(cands, work_blocks, fifo_share, max_iter_trials)) {
+            HostJob& j = jobs[g.id];
+            grants.push_back(Grant{j.slot, uint32_t(g.trials)});
+            grant_jobs.push_back(g.id);
+            j.next += g.trials;
         }
         return CMC_OK;
     }

@@ -12,6 +12,7 @@
 #include <thread>
 
 #include "cmc.h"
+#include "cmc_grants.hpp"
 #include "cmc_runner.hpp"
 
 using namespace cmc;
@@ -367,12 +368,64 @@ void check_locks_and_parameters(const fs::path& root) {
 
 }  // namespace
 
+// The serving grant policy (cmc_grants.hpp) without a device.
+void check_grants() {
+    auto total = [](const std::vector<GrantShare>& g) {
+        uint64_t t = 0;
+        for (const GrantShare& x : g) t += x.trials;
+        return t;
+    };
+    auto of = [](const std::vector<GrantShare>& g, uint32_t id) {
+        for (const GrantShare& x : g)
+            if (x.id == id) return x.trials;
+        return uint64_t(0);
+    };
+    // three jobs of 4096 trials (batches of 1024) at 100 blocks per trial;
+    // job 7 arrived first, job 3 last
+    std::vector<GrantCandidate> jobs = {{3, 0, 4096, 10, 100.0, 0.0, 30},
+                                        {5, 0, 4096, 10, 100.0, 0.0, 20},
+                                        {7, 0, 4096, 10, 100.0, 0.0, 10}};
+    // all in arrival order: the step grows to an eighth of the backlog
+    // (153,600 blocks); the oldest takes what one grant holds (a batch), the
+    // next the rest
+    auto g = grant_shares(jobs, 150000, 1.0, 1u << 20);
+    require(of(g, 7) == 1024 && of(g, 5) == 512 && of(g, 3) == 0, "arrival order fills the oldest first");
+    // a grant never crosses a batch boundary, even when more work is asked for
+    jobs[2].next = 1000;
+    g = grant_shares(jobs, 1u << 30, 1.0, 1u << 20);
+    require(of(g, 7) == 24, "a grant stops at the end of its batch");
+    jobs[2].next = 0;
+    // shortest remaining work first when nothing goes in arrival order: job 3
+    // (96 trials left) is served whole, the step (an eighth of the 828,800-
+    // block backlog) gives the rest, 940 trials, to the next shortest
+    jobs[0].next = 4000;
+    g = grant_shares(jobs, 20000, 0.0, 1u << 20);
+    require(of(g, 3) == 96 && of(g, 7) + of(g, 5) == 940, "shortest remaining work goes first");
+    // the trial cap holds
+    g = grant_shares(jobs, 1u << 30, 0.5, 300);
+    require(total(g) == 300, "no more than max_trials in one step");
+    // a step covers 2.5x the slowest trial's latency even if less was asked
+    std::vector<GrantCandidate> slow = {{1, 0, 1u << 16, 16, 10.0, 4000.0, 1}};
+    g = grant_shares(slow, 10, 1.0, 1u << 20);
+    require(of(g, 1) == 1000, "the step is at least 2.5x one trial's latency");
+    // heaviest trials first in the table
+    std::vector<GrantCandidate> mix = {{1, 0, 64, 6, 10.0, 0.0, 1}, {2, 0, 64, 6, 1000.0, 0.0, 2},
+                                       {3, 0, 64, 6, 100.0, 0.0, 3}};
+    g = grant_shares(mix, 1u << 30, 0.95, 1u << 20);
+    require(g.size() == 3 && g[0].id == 2 && g[1].id == 3 && g[2].id == 1, "heaviest trials first");
+    // a finished job gets nothing
+    mix[1].next = mix[1].budget;
+    g = grant_shares(mix, 1u << 30, 0.95, 1u << 20);
+    require(of(g, 2) == 0 && g.size() == 2, "no trials past a budget");
+}
+
 int main(int argc, char** argv) {
     try {
         const fs::path base = fs::absolute(argc > 1 ? argv[1] : "host_test_data");
         const fs::path root = base / ("run_" + std::to_string(steady_ns()));
         fs::create_directories(root);
         check_keys();
+        check_grants();
         check_pause(root);
         check_journals(root);
         check_k_extension(root);
