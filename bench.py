@@ -167,7 +167,7 @@ def host_threads() -> int:
 def cpu_run(n_trials: int, batch: int, threads: int, w: dict = WORKLOAD):
     """Trials [0, n) of `batch` on the CPU: the reference's own cpu_batch_launch
     (oracle/_ref) when built here, else the oracle restatement.  Returns
-    (seconds, kind, failures)."""
+    (seconds, kind, sorted failing offsets)."""
     lib = reference_lib()
     out = (ctypes.c_uint32 * max(n_trials, 1))()
     t0 = time.perf_counter()
@@ -176,6 +176,7 @@ def cpu_run(n_trials: int, batch: int, threads: int, w: dict = WORKLOAD):
         n = lib.ref_batch_launch(w["mode"].encode(), w["input_mode"].encode(), w["pnum"],
                                  w["ell_i"], w["buckets"], w["kick"], w["seed"], batch, n_trials,
                                  threads, out, ctypes.byref(used))
+        failures = list(out[:n])
         kind = "reference"
     else:
         sys.path.insert(0, str(ROOT / "tests"))
@@ -183,28 +184,55 @@ def cpu_run(n_trials: int, batch: int, threads: int, w: dict = WORKLOAD):
         o = Oracle()
         p = o.params(w["mode"], w["pnum"], w["ell_i"], w["k"], w["buckets"], w["kick"],
                      w["input_mode"])
-        n = len(o.batch(p, w["seed"], batch, 0, n_trials, threads))
+        failures = o.batch(p, w["seed"], batch, 0, n_trials, threads)
         kind = "port"
-    return time.perf_counter() - t0, kind, n
+    return time.perf_counter() - t0, kind, failures
 
 
-def cpu_sample_size(threads: int, target_seconds: float, w: dict = WORKLOAD) -> tuple[int, float, str]:
-    """Grow the sample until one run takes about target_seconds (cap 2^20)."""
+def cpu_sample_size(threads: int, target_seconds: float,
+                    w: dict = WORKLOAD) -> tuple[int, float, str, list]:
+    """Grow the sample until one run takes about target_seconds (cap 2^20);
+    returns (trials, seconds, kind, failures) of the last run."""
     n = max(256, threads * 16) if w["pnum"] < 4096 else threads * 2
     while True:
-        secs, kind, _ = cpu_run(n, 0, threads, w)
+        secs, kind, failures = cpu_run(n, 0, threads, w)
         if secs >= target_seconds * 0.5 or n >= 1 << 20:
-            return n, secs, kind
+            return n, secs, kind, failures
         n = int(min(1 << 20, max(2 * n, n * target_seconds / max(secs, 1e-3))))
 
 
-def cpu_baseline(target_seconds: float = 10.0, w: dict = WORKLOAD) -> dict:
+def cpu_baseline(target_seconds: float = 10.0, w: dict = WORKLOAD) -> tuple[dict, int, list]:
+    """The timed CPU sample: its JSON object, its size n and its failing offsets
+    (the first n trials of batch 0)."""
     threads = host_threads()
-    n, secs, kind = cpu_sample_size(threads, target_seconds, w)
+    n, secs, kind, failures = cpu_sample_size(threads, target_seconds, w)
     return {"value": n / secs, "unit": "trials/s", "cores": threads, "kind": kind,
             "sample": f"first {n} trials of batch 0 of the bench workload "
                       f"({'reference cpu_batch_launch, AES-NI' if kind == 'reference' else 'oracle port'}, "
-                      f"{threads} threads, {secs:.1f} s)"}
+                      f"{threads} threads, {secs:.1f} s)"}, n, failures
+
+
+def parity_check(ctx, cmc, w: dict, n: int, cpu_failures: list, kind: str) -> dict:
+    """The GPU on the CPU sample's trials (batch 0, offsets 0..n-1): both
+    failure lists, compared offset by offset."""
+    p = cmc.parameters(w["mode"], w["pnum"], w["ell_i"], w["k"], w["buckets"], w["kick"],
+                       w["input_mode"])
+    gpu = ctx.launch(p, cmc.batch_key(w["seed"], 0), 0, n)
+    return {"trials": n, "batch": 0, "cpu": kind, "cpu_failures": len(cpu_failures),
+            "gpu_failures": len(gpu), "equal": gpu == cpu_failures}
+
+
+def stressed_parity(ctx, cmc, w: dict, trials: int = 1 << 18) -> dict:
+    """The bench shape with fewer buckets (B = 1250 for t = 1024) and half the
+    eviction limit, where about 1 % of trials fail: the reference's CPU code
+    and the GPU on the same trials, failure lists compared."""
+    ws = dict(w, buckets=int(w["buckets"] * 1250 // 1536), kick=max(1, w["kick"] // 2))
+    secs, kind, failures = cpu_run(trials, 0, host_threads(), ws)
+    out = parity_check(ctx, cmc, ws, trials, failures, kind)
+    out["shape"] = f"t={ws['pnum']}, N=2^{ws['ell_i']}, k={ws['k']}, B={ws['buckets']}, " \
+                   f"kick={ws['kick']}, seed {ws['seed']}"
+    out["cpu_seconds"] = secs
+    return out
 
 
 # ------------------------------------------------------------- replicas --
@@ -234,7 +262,7 @@ def run_reference_arm(args, rank: int, world: int) -> None:
     threads = host_threads()
     w = WORKLOADS.get(args.workload, WORKLOAD)
     # bounded sample per step: about 2 s of CPU work each
-    per_step, _, kind = cpu_sample_size(threads, 2.0, w)
+    per_step, _, kind, _ = cpu_sample_size(threads, 2.0, w)
     for s in range(args.warmup):
         cpu_run(per_step, s, threads, w)
     total = 0.0
@@ -255,6 +283,105 @@ def run_reference_arm(args, rank: int, world: int) -> None:
         "e2e": {"value": value, "unit": "trials/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------- reference arm on the GPU --
+
+def reference_gpu_lib():
+    """The reference's own CUDA driver and kernels (oracle/_ref/librefgpu.so,
+    built unmodified from its sources for sm_100a), or None."""
+    path = ROOT / "oracle" / "_ref" / "librefgpu.so"
+    if not path.exists():
+        return None
+    lib = ctypes.CDLL(str(path))
+    u32, u64, P = ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER
+    lib.ref_gpu_run.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, u32, u32, u32, u32,
+                                u64, u32, u32, ctypes.c_char_p, ctypes.c_char_p,
+                                P(ctypes.c_double), P(u64), P(u64), ctypes.c_char_p, u32]
+    lib.ref_gpu_run.restype = ctypes.c_int
+    return lib
+
+
+def reference_gpu_batch(lib, w: dict, seed: int, bt: int, layout: str = "auto"):
+    """Batch 0 (2^bt trials) of the experiment through the reference's stock
+    GPU worker, with B and the eviction limit of `w`.  Returns (seconds,
+    sorted failing offsets, layout description)."""
+    import tempfile
+    with tempfile.TemporaryDirectory(prefix="cmc-refgpu-") as d:
+        secs, done, failed = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_uint64()
+        info = ctypes.create_string_buffer(256)
+        rc = lib.ref_gpu_run(0, w["mode"].encode(), w["input_mode"].encode(), w["pnum"],
+                             w["ell_i"], w["buckets"], w["kick"], seed, bt, bt, layout.encode(),
+                             d.encode(), ctypes.byref(secs), ctypes.byref(done),
+                             ctypes.byref(failed), info, 256)
+        if rc:
+            raise RuntimeError(f"reference GPU run failed: {info.value.decode()}")
+        rows = (Path(d) / "failures.csv").read_text().split()[1:]
+        offsets = sorted(int(r.split(",")[1]) for r in rows)
+    assert len(offsets) == failed.value and done.value == 1 << bt
+    return secs.value, offsets, info.value.decode()
+
+
+def failure_digest(lists) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for f in lists:
+        h.update(",".join(map(str, f)).encode() + b";")
+    return h.hexdigest()[:16]
+
+
+def run_reference_gpu_arm(args, rank: int, world: int) -> None:
+    """The reference's own CUDA kernels (the plain one-configuration-per-launch
+    GPU form) on this arm's workload: batch 0 of each step's experiment through
+    its stock gpu_worker, timed like its work_elapsed_seconds."""
+    if rank != 0:
+        return
+    lib = reference_gpu_lib()
+    if lib is None:
+        print(json.dumps({"impl": "reference", "ref_device": "gpu",
+                          "unavailable": "oracle/_ref/librefgpu.so not built "
+                                         "(make -C oracle refgpu REF=<reference dir>)"}))
+        return
+    if args.workload == "sweep":
+        n = args.sweep_trials
+        bt = n.bit_length() - 1
+        assert n == 1 << bt, "--sweep-trials must be a power of two for the reference worker"
+        sets = [s for s in sweep_sets() if s["k"] == 3]   # the reference hard-codes k = 3
+        total, lists, per_set = 0.0, [], []
+        for s in sets:
+            secs, fails, info = reference_gpu_batch(lib, s, s["seed"], bt)
+            total += secs
+            lists.append(fails)
+            per_set.append({"t": s["pnum"], "B": s["buckets"], "kick": s["kick"],
+                            "trials_per_s": n / secs, "failures": len(fails), "plan": info})
+        line = {"impl": "reference", "ref_device": "gpu",
+                "metric": "sweep trials/s, k = 3 sets (bit-exact failures)",
+                "value": n * len(sets) / total, "unit": "trials/s", "sets": len(sets),
+                "trials_per_set": n, "seconds": total, "failures": sum(map(len, lists)),
+                "failures_digest": failure_digest(lists), "per_set": per_set,
+                "timing": "host wall clock around the reference's gpu_worker per set"}
+        print(json.dumps(line), flush=True)
+        return
+    w = WORKLOADS.get(args.workload, WORKLOAD)
+    bt = min(w["bt"], (w["trials"] - 1).bit_length())
+    for _ in range(args.warmup):
+        reference_gpu_batch(lib, w, w["seed"], bt)
+    total, info, fails = 0.0, "", []
+    for _ in range(args.steps):
+        secs, fails, info = reference_gpu_batch(lib, w, w["seed"], bt)
+        total += secs
+    value = (1 << bt) * args.steps / total
+    line = {"impl": "reference", "ref_device": "gpu", "metric": METRIC, "value": value,
+            "unit": "trials/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "dtype": "u32", "data": "synthetic (seeded AES-CTR trial stream)",
+            "config": {"workload": w["workload"], "trials_per_step": 1 << bt,
+                       "batch": 0, "plan": info},
+            "failures": len(fails), "failures_digest": failure_digest([fails]),
+            "timing": "host wall clock around the reference's gpu_worker (its "
+                      "work_elapsed_seconds): allocation, launches, per-launch read-back, "
+                      "journal commit"}
     print(json.dumps(line), flush=True)
 
 
@@ -279,13 +406,17 @@ def sweep_sets(n_sets: int = 64, draw_seed: int = 3):
 
 
 def run_sweep_workload(args):
-    """Plain (one launch per parameter set) vs batched (all sets in one
-    persistent launch) on the mixed sweep; both must give identical failures."""
-    import torch
     cmc = load_pkg()
     ctx = cmc.Context(0)
+    print(json.dumps(sweep_measure(cmc, ctx, args.sweep_trials)), flush=True)
+    ctx.close()
+
+
+def sweep_measure(cmc, ctx, n: int) -> dict:
+    """Plain (one launch per parameter set) vs batched (all sets in one call)
+    on the mixed sweep; both must give identical failures."""
+    import torch
     sets = sweep_sets()
-    n = args.sweep_trials
     params = [cmc.parameters(s["mode"], s["pnum"], s["ell_i"], s["k"], s["buckets"], s["kick"],
                              s["input_mode"]) for s in sets]
     jobs = [(p, s["seed"], 0, 0, n) for p, s in zip(params, sets)]
@@ -327,8 +458,7 @@ def run_sweep_workload(args):
         "mean_aes_blocks_per_trial": avg_blocks, "tuned_plan": choice,
         "timing": "host wall clock around synchronous C-ABI calls (cmc_launch / cmc_run_jobs)",
     }
-    print(json.dumps(line), flush=True)
-    ctx.close()
+    return line
 
 
 # ------------------------------------------------------------ serve workload --
@@ -363,10 +493,15 @@ def rounded_budget(trials: int, bt_max: int = 20):
 
 
 def run_serve_workload(args):
-    """Served (continuous batching) vs plain (one launch per job, in arrival
-    order) on the same job stream; job latency = completion - arrival."""
     cmc = load_pkg()
     ctx = cmc.Context(0)
+    print(json.dumps(serve_measure(cmc, ctx, args)), flush=True)
+    ctx.close()
+
+
+def serve_measure(cmc, ctx, args) -> dict:
+    """Served (continuous batching) vs plain (one launch per job, in arrival
+    order) on the same job stream; job latency = completion - arrival."""
     lo, hi = (float(x) for x in args.serve_log2_budget.split(","))
     jobs = serve_jobs(args.serve_jobs, args.serve_rate, (lo, hi))
     params = [cmc.parameters(j["mode"], j["pnum"], j["ell_i"], j["k"], j["buckets"], j["kick"],
@@ -442,8 +577,7 @@ def run_serve_workload(args):
         "fifo_share": args.serve_fifo_share, "resident": args.serve_resident,
         "timing": "host wall clock from each job's arrival to its completion",
     }
-    print(json.dumps(line), flush=True)
-    ctx.close()
+    return line
 
 
 # ------------------------------------------------------------------ our arm --
@@ -454,7 +588,12 @@ def main():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ref-device", choices=["cpu", "gpu"], default="cpu",
+                    help="--impl reference: the reference's CPU path (default) or its own CUDA "
+                         "kernels built for sm_100a (the plain GPU form)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload only: skip the sweep and serve objects")
     ap.add_argument("--trials", type=int, default=0,
                     help="trials per step (default: the workload's, 2^20 for config2); "
                          "smaller for profiling")
@@ -476,7 +615,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
-        run_reference_arm(args, rank, world)
+        if args.ref_device == "gpu":
+            run_reference_gpu_arm(args, rank, world)
+        else:
+            run_reference_arm(args, rank, world)
         return
     if args.workload == "sweep":
         if rank == 0:
@@ -606,7 +748,21 @@ def main():
             "clocks": clk,
         }
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline(w=w)
+            base, n_cpu, cpu_fails = cpu_baseline(w=w)
+            line["cpu_baseline"] = base
+            line["parity"] = parity_check(ctx, cmc, w, n_cpu, cpu_fails, base["kind"])
+            if args.workload == "config2":
+                line["parity_stressed"] = stressed_parity(ctx, cmc, w)
+        if world == 1 and args.workload == "config2" and not args.no_extras:
+            # the batching and serving patterns, measured on the same box after
+            # the timed region (own contexts; bounded to about a minute each)
+            for name, fn in (("sweep", lambda c: sweep_measure(cmc, c, args.sweep_trials)),
+                             ("serve", lambda c: serve_measure(cmc, c, args))):
+                c2 = cmc.Context(local)
+                try:
+                    line[name] = fn(c2)
+                finally:
+                    c2.close()
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

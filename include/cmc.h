@@ -213,9 +213,11 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
  * that must not pay cudaMalloc/cudaFree's device-wide synchronisation.  Same
  * result as cmc_launch_device, on the current device, with no context and no
  * allocation: the working memory is a fixed file-scope device array (about
- * 129 KiB per GPU, held until the process exits).  Limits: count is 1..2^20
- * trials per call, and parameter sets whose walk slots do not fit in shared
- * memory are rejected (CMC_EINVAL).  d_batch_key, d_out_offsets (capacity
+ * 129 KiB per GPU, held until the process exits).  Limits: count is 0..2^20
+ * trials per call (0 writes *d_out_nfailed = 0, as cmc_launch_device does),
+ * and parameter sets whose walk slots do not fit in shared memory are
+ * rejected (CMC_EINVAL): among them every set that needs 32-bit table entries
+ * (B > 65535 or t > 16384), whose bins and map exceed shared memory.  d_batch_key, d_out_offsets (capacity
  * count) and d_out_nfailed are device pointers; work is queued on `stream`.
  * The first call on a device sets up that device (symbol addresses, a 1 KiB
  * table upload), so it should come before any stream capture.  All calls on a

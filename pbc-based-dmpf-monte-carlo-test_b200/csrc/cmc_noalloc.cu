@@ -152,8 +152,8 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
     using namespace cmc;
     if (!params || !d_batch_key || !d_out_offsets || !d_out_nfailed)
         return fail(CMC_EINVAL, "cmc_launch_static: null argument");
-    if (count == 0 || count > kStaticMaxTrials)
-        return fail(CMC_EINVAL, "cmc_launch_static: count must be 1.." + std::to_string(kStaticMaxTrials) +
+    if (count > kStaticMaxTrials)
+        return fail(CMC_EINVAL, "cmc_launch_static: count must be at most " + std::to_string(kStaticMaxTrials) +
                                     " (the fixed working memory holds that many trials per call)");
     if (uint64_t(first) + count > 0x100000000ULL)
         return fail(CMC_EINVAL, "cmc_launch_static: offset range overflows");
@@ -164,6 +164,11 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
     DeviceState* st = nullptr;
     int rc = setup(device, st);
     if (rc) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (count == 0) {  // as cmc_launch_device: no trials, no failures
+        const cudaError_t e = cudaMemsetAsync(d_out_nfailed, 0, sizeof(uint32_t), s);
+        return e == cudaSuccess ? CMC_OK : fail(CMC_ECUDA, std::string("memset count: ") + cudaGetErrorString(e));
+    }
     Ctx& pl_ctx = *st->planner;
     Job& job = st->jobs[0];
     if ((rc = pl_ctx.make_job(*params, first, count, 0, job))) return fail(rc, pl_ctx.err);
@@ -173,8 +178,10 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
         return fail(CMC_EINVAL,
                     "cmc_launch_static: these parameters need walk slots in global memory, which "
                     "would be an allocation; use cmc_launch_device");
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const uint32_t words = (count + 31) / 32;
+    // the launch checks below read cudaGetLastError: an earlier non-fatal
+    // error of the caller's is not this call's
+    cudaGetLastError();
     static_prepare<<<64, 256, 0, s>>>(job, d_batch_key, st->scratch, words);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(CMC_ECUDA, std::string("prepare launch: ") + cudaGetErrorString(e));

@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Generate tests/golden/golden.json from the reference.
 
-Sources (read from the reference tree, default /root/reference):
+Sources (read from the reference tree, given with --ref):
   * cpu_golden.hpp:3-4        -- 32,768-trial failure lists (seed 123, PNUM 16, ell_i 8,
                                  ET 15, BT 8, sequential) for BGH25 and DRRT18
   * smoke_expected.json        -- the first 8,192 trials of the same set
@@ -15,7 +15,7 @@ into oracle/_ref/libcmcref.so (oracle/Makefile target `ref`): cpu_trial
 parameters() over a grid, and batch_key() schedules.
 
 The JSON is committed; tests never read the reference tree.
-Usage: python tests/golden/make_golden.py [--ref /root/reference]
+Usage: python tests/golden/make_golden.py --ref <directory of the reference sources>
 """
 import argparse
 import ctypes
@@ -33,7 +33,7 @@ def ints(text):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="directory of the reference sources")
     args = ap.parse_args()
     ref = Path(args.ref)
     subprocess.run(["make", "-C", str(ROOT / "oracle"), "all", "ref", f"REF={ref}"], check=True,

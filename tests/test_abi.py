@@ -22,10 +22,14 @@ def test_exports_every_declared_symbol(cmc):
     assert set(declared) == set(cmc.EXPORTS)
 
 
-def test_library_targets_sm100a(cmc):
-    # the device code is compiled for sm_100a only (no PTX, no other arch)
-    blob = cmc.LIB_PATH.read_bytes()
-    assert b"sm_100a" in blob
+def test_build_targets_sm100a_only():
+    # every nvcc line of the product build compiles for sm_100a and nothing else
+    # (no PTX for JIT, no other architecture)
+    make = (ROOT / "pbc-based-dmpf-monte-carlo-test_b200" / "Makefile").read_text()
+    arch = re.findall(r"^ARCH\s*:=\s*(.+)$", make, re.M)
+    assert arch == ["-gencode arch=compute_100a,code=sm_100a"]
+    assert "$(ARCH)" in make.split("CUFLAGS", 1)[1].split("\n", 1)[0]
+    assert re.findall(r"-arch[= ]|compute_\d+(?![\da])|code=compute", make) == []
 
 
 def test_params_grid(cmc, golden):
