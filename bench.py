@@ -447,6 +447,17 @@ def sweep_measure(cmc, ctx, n: int) -> dict:
     graph_state = ctx.last_plan.rsplit("graph=", 1)[-1] if "graph=" in ctx.last_plan else "off"
     same = same and tuned == ref
     avg_blocks = sum(algorithmic_blocks(p) for p in params) / len(params)
+    # the k = 3 sets alone: the sets the reference's kernels can run
+    # (bench.py --impl reference --ref-device gpu --workload sweep times them)
+    k3 = [i for i, st in enumerate(sets) if st["k"] == 3]
+    k3_jobs = [jobs[i] for i in k3]
+    ctx.run_jobs(k3_jobs)
+    ctx.run_jobs(k3_jobs)
+    t0 = time.perf_counter(); ctx.run_jobs(k3_jobs); t_k3 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for i in k3:
+        ctx.launch(params[i], cmc.batch_key(sets[i]["seed"], 0), 0, n)
+    t_k3_plain = time.perf_counter() - t0
     line = {
         "metric": "sweep trials/s (64 mixed parameter sets, bit-exact failures)",
         "workload": f"sweep: 64 sets drawn with seed 3, {n} trials each (batch 0, offsets 0..{n - 1})",
@@ -456,6 +467,10 @@ def sweep_measure(cmc, ctx, n: int) -> dict:
         "identical_failures": same, "failures": sum(len(f) for f in ref),
         "batched_graph": graph_state,
         "mean_aes_blocks_per_trial": avg_blocks, "tuned_plan": choice,
+        "k3_sets": {"sets": len(k3), "batched_trials_per_s": n * len(k3) / t_k3,
+                    "plain_trials_per_s": n * len(k3) / t_k3_plain,
+                    "failures": sum(len(ref[i]) for i in k3),
+                    "failures_digest": failure_digest([ref[i] for i in k3])},
         "timing": "host wall clock around synchronous C-ABI calls (cmc_launch / cmc_run_jobs)",
     }
     return line
