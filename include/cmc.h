@@ -103,7 +103,10 @@ typedef struct cmc_job {
 
 /* Batched form (no counterpart in the reference, which runs one parameter set
  * per process): all jobs in ONE persistent engine launch, heavy jobs first so
- * uneven table sizes balance across SMs.  out_failed[j] receives the number of
+ * uneven table sizes balance across SMs.  Jobs whose best plans differ (walk
+ * slots in shared or global memory, warps per group, entry width, cache kind)
+ * form plan classes; each CTA runs one class at a time under that class's plan
+ * and moves on to the class with the most work left when its own runs out.  out_failed[j] receives the number of
  * failing trials of job j.  If out_offsets is not NULL, the failing offsets are
  * written job by job in ascending order, out_jobs[i] (if not NULL) naming the
  * job of out_offsets[i]; cap is their capacity and *out_total the number of
@@ -203,7 +206,12 @@ int cmc_server_destroy(cmc_server* server);
  * "graph" (1, the default: cmc_run_jobs captures the device side of a call shape -- job shapes, counts and buffers -- into a CUDA
  * graph on its second call and replays it from the third; 0: always eager),
  * "map_chains" (0 automatic, or 1, 2, 4, 8: candidate lookup chains per lane
- * when a bucket map is built from a round cache).
+ * when a bucket map is built from a round cache), "fused" (1, the default:
+ * the plan classes of a batched call run in one persistent launch whose CTAs
+ * move to the class with the most work left; 0: one launch per class),
+ * "fill_blocks" (0 automatic, or 2..4: AES blocks each thread keeps in flight
+ * while filling a round cache, in plans whose walk slots are in shared
+ * memory; automatic is 3 there and 2 elsewhere).
  * Returns CMC_EINVAL for an unknown name or a value out of range. */
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
 

@@ -169,17 +169,26 @@ __device__ __forceinline__ void prp_key_from_schedule(const uint32_t* rk, PrpKey
     k.k43lo = rk[43] & 0xffffu;
 }
 
-// Low 16 bits of AES_k(0x43455350, r, h, R).w3 for R < 2^16.
-__device__ __forceinline__ uint32_t prp_f(const Lanes& L, const PrpKey& k, const Round1& c,
-                                          uint32_t R) {
+// State after AES round 2 of AES_k(0x43455350, r, h, R) for R < 2^16.
+__device__ __forceinline__ void round2_state(const Lanes& L, const PrpKey& k, const Round1& c,
+                                             uint32_t R, uint32_t t[4]) {
     const uint32_t w3 = R ^ c.w3hi;
     // round 1: t0 = c0 ^ Te3[w3 b0], t1 = c1 ^ Te2[w3 b1], t2 = c2, t3 = c3
-    uint32_t s0 = c.c0 ^ ror8(lds(toff<0>(w3, L.lb2)));
-    uint32_t s1 = c.c1 ^ lds(toff<1>(w3, L.lb2));
-    uint32_t s2 = c.c2, s3 = c.c3;
-    // rounds 2..8
+    const uint32_t s0 = c.c0 ^ ror8(lds(toff<0>(w3, L.lb2)));
+    const uint32_t s1 = c.c1 ^ lds(toff<1>(w3, L.lb2));
+    const uint32_t s2 = c.c2, s3 = c.c3;
+    t[0] = column(L, s0, s1, s2, s3, k.kr[0]);
+    t[1] = column(L, s1, s2, s3, s0, k.kr[1]);
+    t[2] = column(L, s2, s3, s0, s1, k.kr[2]);
+    t[3] = column(L, s3, s0, s1, s2, k.kr[3]);
+}
+
+// Rounds 3..10 from the state after round 2; low 16 bits of w3.
+__device__ __forceinline__ uint32_t prp_tail(const Lanes& L, const PrpKey& k, uint32_t s0,
+                                             uint32_t s1, uint32_t s2, uint32_t s3) {
+    // rounds 3..8
 #pragma unroll
-    for (int r = 0; r < 7; ++r) {
+    for (int r = 1; r < 7; ++r) {
         const uint32_t t0 = column(L, s0, s1, s2, s3, k.kr[4 * r + 0]);
         const uint32_t t1 = column(L, s1, s2, s3, s0, k.kr[4 * r + 1]);
         const uint32_t t2 = column(L, s2, s3, s0, s1, k.kr[4 * r + 2]);
@@ -193,6 +202,49 @@ __device__ __forceinline__ uint32_t prp_f(const Lanes& L, const PrpKey& k, const
     const uint32_t hi = lds(toff<1>(u1, L.lb0));  // T0: S at bits 8..15
     const uint32_t lo = lds(toff<0>(u2, L.lb2));  // T2: S at bits 0..7
     return ((hi & 0xff00u) | (lo & 0x00ffu)) ^ k.k43lo;
+}
+
+// Low 16 bits of AES_k(0x43455350, r, h, R).w3 for R < 2^16.
+__device__ __forceinline__ uint32_t prp_f(const Lanes& L, const PrpKey& k, const Round1& c,
+                                          uint32_t R) {
+    uint32_t t[4];
+    round2_state(L, k, c, R, t);
+    return prp_tail(L, k, t[0], t[1], t[2], t[3]);
+}
+
+// Round-2 fold.  For one trial key and Feistel round r, byte 0 of w3 = R ^ rk3
+// enters round 1 only through state word 0 and byte 1 only through word 1
+// (round2_state above), and round 2 is linear in its input columns' table
+// outputs.  So the state after round 2 is U(w3 b0) ^ V(w3 b1) with
+//   U(a) = (Te0[s0 b3], Te3[s0 b0], Te2[s0 b1], Te1[s0 b2]),  s0 = c0 ^ Te3[a]
+// (the round-2 lookups that read word 0) and V holding the rest, round keys
+// included.  V depends on R only through R >> 8 (R < 2^16): a table of
+// 2^max(0, h-8) entries per round, built once per trial by fold_entry; the
+// round cache fill then spends 5 lookups on rounds 1 and 2 instead of 18.
+__device__ __forceinline__ void round2_u(const Lanes& L, uint32_t c0, uint32_t w3, uint32_t u[4]) {
+    const uint32_t s0 = c0 ^ ror8(lds(toff<0>(w3, L.lb2)));
+    u[0] = lds(top_byte_off(L, s0));
+    u[1] = ror8(lds(toff<0>(s0, L.lb2)));
+    u[2] = lds(toff<1>(s0, L.lb2));
+    u[3] = ror8(lds(toff<2>(s0, L.lb0)));
+}
+
+// V entry for the R values with R >> 8 == y: the state after round 2 of
+// R = y << 8 | (rk3 & 255) (so that w3 b0 = 0) with U(0) removed.
+__device__ __forceinline__ uint4 fold_entry(const Lanes& L, const PrpKey& k, const Round1& c,
+                                            uint32_t y) {
+    uint32_t t[4], u[4];
+    round2_state(L, k, c, (y << 8) | (c.w3hi & 255u), t);
+    round2_u(L, c.c0, 0u, u);
+    return make_uint4(t[0] ^ u[0], t[1] ^ u[1], t[2] ^ u[2], t[3] ^ u[3]);
+}
+
+// prp_f through the fold: v = the V entry of R >> 8 for this round.
+__device__ __forceinline__ uint32_t prp_f_folded(const Lanes& L, const PrpKey& k, uint32_t c0,
+                                                 uint32_t w3hi, const uint4& v, uint32_t R) {
+    uint32_t u[4];
+    round2_u(L, c0, R ^ w3hi, u);
+    return prp_tail(L, k, u[0] ^ v.x, u[1] ^ v.y, u[2] ^ v.z, u[3] ^ v.w);
 }
 
 // Full 32-bit w3 of AES_k(0x43455350, r, h, R) for any 32-bit R (h > 16),

@@ -17,10 +17,12 @@
 
 namespace cmc {
 
-template <typename MapT, typename BinT, bool WIDE>
+template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
 __global__ void cmc_engine(const EngineArgs a);
 template <typename MapT, typename BinT, bool WIDE>
 __global__ void cmc_engine_split(const EngineArgs a);
+template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
+__global__ void cmc_engine_fused(const __grid_constant__ FusedArgs f);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
                                      uint32_t* out, uint32_t* count, uint64_t cap,
                                      const unsigned long long* nbits_dev);
@@ -150,8 +152,11 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     pl.bins_bytes = round_up(max_b * entry, 16);
     const uint32_t map_bytes = round_up(max_cand * entry, 16);
     pl.slot_stride = round_up(pl.bins_bytes + map_bytes, 128);
-    const uint32_t cache_bytes = any_cache ? (16u << max_cache_h) : 0;
-    pl.group_bytes = kGroupHeaderBytes + cache_bytes;
+    // a round-cache job keeps its fold table (and a shared-memory cache) in
+    // its group's shared region
+    const uint32_t cache_bytes = any_cache ? fold_table_bytes(max_cache_h) + (16u << max_cache_h) : 0;
+    const uint32_t gfold_bytes = any_gcache ? fold_table_bytes(max_gcache_h) : 0;
+    pl.group_bytes = kGroupHeaderBytes + std::max(cache_bytes, gfold_bytes);
     const double avg_cand = work > 0 ? cand_work / work : 0;
     pl.wg = (any_cache || any_gcache || avg_cand >= 768.0) ? 4 : 1;
     if (force_wg) pl.wg = force_wg;
@@ -271,30 +276,49 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     const uint32_t nclass = uint32_t(bounds.size()) - 1;
     if (nclass < 1 || nclass > kMaxClasses) return fail(CMC_EINVAL, "bad plan classes");
     std::vector<Plan> plans(nclass);
-    uint64_t pool = 0;
+    std::vector<double> class_work(nclass, 0.0), class_trials(nclass, 0.0);
     uint32_t heaviest = 0;
     uint64_t heaviest_trials = 0;
+    bool any_split = false;
     std::string text;
     for (uint32_t c = 0; c < nclass; ++c) {
         std::vector<Job> part(jobs.begin() + bounds[c], jobs.begin() + bounds[c + 1]);
         int rc = plan(part, plans[c]);
         if (rc) return rc;
-        const Plan& pl = plans[c];
-        pool = std::max<uint64_t>(pool, (pl.gslot_bytes + 255) / 256 * 256 + pl.gcache_bytes);
+        any_split = any_split || plans[c].walker_ctas;
         uint64_t trials = 0;
-        for (const Job& j : part) trials += j.count;
+        for (const Job& j : part) {
+            trials += j.count;
+            class_work[c] += job_cost(j) * j.count;
+        }
+        class_trials[c] = double(trials);
         if (trials > heaviest_trials) {
             heaviest_trials = trials;
             heaviest = c;
         }
         text += (c ? " | " : "") + plan_text;
     }
-    plan_text = text;
+    // Several classes run as ONE persistent launch unless disabled or a class
+    // uses the split engine; the classes then run side by side, so each gets
+    // its own region of the global pool.  Launches one after another reuse one
+    // region in stream order.
+    const bool fuse = use_fused && nclass > 1 && nclass <= kMaxFusedClasses && !any_split;
+    std::vector<uint64_t> region(nclass, 0);
+    uint64_t pool = 0;
+    for (uint32_t c = 0; c < nclass; ++c) {
+        const uint64_t need = (plans[c].gslot_bytes + 255) / 256 * 256 + (plans[c].gcache_bytes + 255) / 256 * 256;
+        if (fuse) {
+            region[c] = pool;
+            pool += need;
+        } else {
+            pool = std::max(pool, need);
+        }
+    }
+    plan_text = fuse ? "fused(" + std::to_string(nclass) + ") " + text : text;
     const size_t words = (total + 31) / 32;
     int rc = grow(d_bits, bits_cap, words, "failure bitmap");
     if (rc) return rc;
-    // one global pool per launch, reused by the classes in stream order:
-    // walk slots, then the groups' round caches
+    // walk slots, then the groups' round caches, per pool region
     if (pool && (rc = grow(d_slots, slots_cap, size_t(pool), "slot and cache pool"))) return rc;
     if ((rc = cuda(cudaMemsetAsync(d_ctrl, 0, nclass * sizeof(Ctrl), st), "memset ctrl"))) return rc;
     if ((rc = cuda(cudaMemsetAsync(d_bits, 0, words * 4, st), "memset bitmap"))) return rc;
@@ -302,13 +326,9 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
     // around the graph launch instead
     if (!capturing && (rc = cuda(cudaEventRecord(ev_start, st), "event"))) return rc;
     kernels = 0;
-    for (uint32_t c = 0; c < nclass; ++c) {
+    auto class_args = [&](uint32_t c) {
         const Plan& pl = plans[c];
-        if (pl.walker_ctas) {
-            if ((rc = grow(d_ghdr, ghdr_cap, pl.ns, "slot headers"))) return rc;
-            if ((rc = cuda(cudaMemsetAsync(d_ghdr, 0, size_t(pl.ns) * sizeof(GSlotHeader), st), "memset slots")))
-                return rc;
-        }
+        char* base = d_slots + region[c];
         const size_t cache_off = size_t((pl.gslot_bytes + 255) / 256 * 256);
         EngineArgs a{};
         a.jobs = d_jobs;
@@ -319,8 +339,8 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
         a.fail_bits = d_bits;
         a.job_failed = job_failed;
         a.job_done = job_done;
-        a.gslots = pl.slots_smem ? nullptr : d_slots;
-        a.gcache = pl.gcache_bytes ? reinterpret_cast<uint16_t*>(d_slots + cache_off) : nullptr;
+        a.gslots = pl.slots_smem ? nullptr : base;
+        a.gcache = pl.gcache_bytes ? reinterpret_cast<uint16_t*>(base + cache_off) : nullptr;
         a.gcache_stride = pl.gcache_stride;
         a.ghdr = pl.walker_ctas ? d_ghdr : nullptr;
         a.split = pl.walker_ctas ? 1 : 0;
@@ -341,14 +361,57 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
         a.spin_limit = spin_limit;
         a.idle_polls = spin_limit;
         a.map_chains = map_chains;
+        a.fill_blocks = fill_blocks;
+        return a;
+    };
+    // Fused: one launch per entry width that two or more classes share (the
+    // width is a template parameter of the engine), in the order of each
+    // width's heaviest class; a class alone in its width runs by itself.
+    std::vector<bool> launched(nclass, false);
+    for (uint32_t lead = 0; lead < nclass && fuse; ++lead) {
+        if (launched[lead]) continue;
+        std::vector<uint32_t> members;
+        for (uint32_t c = lead; c < nclass; ++c)
+            if (!launched[c] && plans[c].variant == plans[lead].variant &&
+                plans[c].slots_smem == plans[lead].slots_smem)
+                members.push_back(c);
+        if (members.size() < 2) continue;
+        FusedArgs fa{};
+        fa.nclass = uint32_t(members.size());
+        uint32_t smem = 0;
+        double all = 0, cum = 0;
+        for (uint32_t c : members) all += class_work[c];
+        for (uint32_t i = 0; i < members.size(); ++i) {
+            const uint32_t c = members[i];
+            launched[c] = true;
+            fa.cls[i] = class_args(c);
+            fa.cost[i] = float(class_work[c] / std::max(1.0, class_trials[c]));
+            fa.first_cta[i] = uint16_t(std::lround(double(sms) * cum / std::max(all, 1e-30)));
+            cum += class_work[c];
+            smem = std::max(smem, plans[c].smem_bytes);
+        }
+        fa.first_cta[members.size()] = uint16_t(sms);
+        const void* fn = fused_engine_kernel(plans[lead].variant, plans[lead].slots_smem);
+        void* args[] = {&fa};
+        if ((rc = cuda(cudaLaunchKernel(fn, dim3(sms), dim3(512), args, smem, st), "fused engine launch")))
+            return rc;
+        ++kernels;
+    }
+    for (uint32_t c = 0; c < nclass; ++c) {
+        if (launched[c]) continue;
+        const Plan& pl = plans[c];
+        if (pl.walker_ctas) {
+            if ((rc = grow(d_ghdr, ghdr_cap, pl.ns, "slot headers"))) return rc;
+            if ((rc = cuda(cudaMemsetAsync(d_ghdr, 0, size_t(pl.ns) * sizeof(GSlotHeader), st), "memset slots")))
+                return rc;
+        }
+        EngineArgs a = class_args(c);
         const void* fn =
             pl.walker_ctas
                 ? (pl.variant == 0   ? (const void*)cmc_engine_split<uint16_t, uint16_t, false>
                    : pl.variant == 1 ? (const void*)cmc_engine_split<uint32_t, uint32_t, false>
                                      : (const void*)cmc_engine_split<uint32_t, uint32_t, true>)
-                : (pl.variant == 0   ? (const void*)cmc_engine<uint16_t, uint16_t, false>
-                   : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
-                                     : (const void*)cmc_engine<uint32_t, uint32_t, true>);
+                : engine_kernel(pl.variant, pl.slots_smem);
         void* args[] = {&a};
         // The split engine's producer and walker CTAs hand trials to each other, so
         // they must all be resident at once: a cooperative launch guarantees it.
@@ -396,16 +459,38 @@ int Ctx::check_ctrl() {
     return CMC_OK;
 }
 
+const void* engine_kernel(int variant, bool smem_slots) {
+    if (smem_slots)
+        return variant == 0   ? (const void*)cmc_engine<uint16_t, uint16_t, false, true>
+               : variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false, true>
+                              : (const void*)cmc_engine<uint32_t, uint32_t, true, true>;
+    return variant == 0   ? (const void*)cmc_engine<uint16_t, uint16_t, false, false>
+           : variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false, false>
+                          : (const void*)cmc_engine<uint32_t, uint32_t, true, false>;
+}
+
+const void* fused_engine_kernel(int variant, bool smem_slots) {
+    if (smem_slots)
+        return variant == 0   ? (const void*)cmc_engine_fused<uint16_t, uint16_t, false, true>
+               : variant == 1 ? (const void*)cmc_engine_fused<uint32_t, uint32_t, false, true>
+                              : (const void*)cmc_engine_fused<uint32_t, uint32_t, true, true>;
+    return variant == 0   ? (const void*)cmc_engine_fused<uint16_t, uint16_t, false, false>
+           : variant == 1 ? (const void*)cmc_engine_fused<uint32_t, uint32_t, false, false>
+                          : (const void*)cmc_engine_fused<uint32_t, uint32_t, true, false>;
+}
+
 // Every engine kernel may use up to the device's opt-in shared memory.  Set
 // once per device and never lowered, so launches of different plans -- and
 // graphs captured from them -- are valid whatever ran in between.
 int engine_smem_cap(size_t optin) {
-    const void* fns[] = {(const void*)cmc_engine<uint16_t, uint16_t, false>,
-                         (const void*)cmc_engine<uint32_t, uint32_t, false>,
-                         (const void*)cmc_engine<uint32_t, uint32_t, true>,
+    const void* fns[] = {engine_kernel(0, true), engine_kernel(1, true), engine_kernel(2, true),
+                         engine_kernel(0, false), engine_kernel(1, false), engine_kernel(2, false),
                          (const void*)cmc_engine_split<uint16_t, uint16_t, false>,
                          (const void*)cmc_engine_split<uint32_t, uint32_t, false>,
-                         (const void*)cmc_engine_split<uint32_t, uint32_t, true>};
+                         (const void*)cmc_engine_split<uint32_t, uint32_t, true>,
+                         fused_engine_kernel(0, true), fused_engine_kernel(1, true),
+                         fused_engine_kernel(2, true), fused_engine_kernel(0, false),
+                         fused_engine_kernel(1, false), fused_engine_kernel(2, false)};
     for (const void* fn : fns)
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(optin)) != cudaSuccess)
             return CMC_ECUDA;
@@ -573,10 +658,10 @@ std::string Ctx::graph_key(const std::vector<Job>& jobs, const std::vector<uint3
         key += b;
     }
     for (uint32_t x : bounds) key += std::to_string(x) + ",";
-    snprintf(b, sizeof b, "|%llu|%llu|%u/%u/%u/%u/%u/%d/%d/%d/%u/%u|%p/%p/%p/%p/%p/%p/%p/%p",
+    snprintf(b, sizeof b, "|%llu|%llu|%u/%u/%u/%u/%u/%d/%d/%d/%u/%u/%d|%p/%p/%p/%p/%p/%p/%p/%p",
              (unsigned long long)total, (unsigned long long)dev_cap, force_wg, force_ng,
              force_global_slots, force_walkers, max_slots_per_group, force_walker_ctas, force_isolate,
-             force_method, spin_limit, map_chains, (void*)d_jobs, (void*)d_bits, (void*)d_out, (void*)d_slots,
+             force_method, spin_limit, map_chains * 16 + fill_blocks, use_fused, (void*)d_jobs, (void*)d_bits, (void*)d_out, (void*)d_slots,
              (void*)d_ctrl, (void*)d_job_failed, (void*)h_failed, (void*)h_nf);
     return key + b;
 }
@@ -940,6 +1025,8 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
     else if (n == "method" && value >= -1 && value <= 2) c->force_method = int(value);
     else if (n == "graph" && (value == 0 || value == 1)) c->use_graphs = int(value);
+    else if (n == "fused" && (value == 0 || value == 1)) c->use_fused = int(value);
+    else if (n == "fill_blocks" && (value == 0 || (value >= 2 && value <= 4))) c->fill_blocks = uint32_t(value);
     else if (n == "map_chains" && (value == 0 || value == 1 || value == 2 || value == 4 || value == 8))
         c->map_chains = uint32_t(value);
     else if (n == "walkers" && value >= 0 && value <= 4) c->force_walkers = uint32_t(value);

@@ -12,7 +12,8 @@
 
 namespace cmc {
 
-constexpr uint32_t kMaxClasses = 16;  // plan classes (engine launches) per batched call
+constexpr uint32_t kMaxClasses = 16;  // plan classes per batched call
+static_assert(kMaxClasses <= kMaxFusedClasses, "every class fits a fused launch");
 
 struct Plan {
     uint32_t ng = 0, wg = 0, ns = 0, nw = 1;
@@ -30,6 +31,10 @@ struct Plan {
 uint32_t choose_method(uint32_t h, uint64_t domain, double candidates, int force, bool may_allocate);
 // Raises the engine kernels' dynamic shared-memory limit to the device's opt-in maximum.
 int engine_smem_cap(size_t optin);
+// The engine kernel for a plan's entry width (Plan::variant) and walk-slot
+// placement, and the fused kernel of the same kind.
+const void* engine_kernel(int variant, bool smem_slots);
+const void* fused_engine_kernel(int variant, bool smem_slots);
 // Estimated cost of one trial in AES-block equivalents (seeds, map, 0.1 t for the walk).
 double job_cost(const Job& j);
 
@@ -83,6 +88,7 @@ struct Ctx {
         Plan plan;
     };
     int use_graphs = 1;
+    int use_fused = 1;  // batched calls: all plan classes in one persistent launch
     bool capturing = false;
     std::vector<GraphEntry> graphs;  // most recent last, at most 8
     std::vector<std::string> graph_seen;
@@ -94,6 +100,7 @@ struct Ctx {
     bool may_allocate = true;  // false: no global round cache, global slots only if unavoidable
     uint32_t spin_limit = 1u << 26;
     uint32_t map_chains = 0;  // lookup chains per lane from a round cache (0: automatic)
+    uint32_t fill_blocks = 0; // round-cache fill: independent blocks per thread and step (0: automatic)
 
     ~Ctx();
     int init(int dev);

@@ -41,7 +41,7 @@ struct GroupHeader {
     unsigned long long gidx;
     uint32_t job, offset;
     uint32_t rk[44];
-    uint32_t r1[8][8];  // Round1 {c0, c1, c2, c3, w3hi} per Feistel round (padded)
+    uint32_t r1[8][8];  // Round1 {c0, w3hi, c1, c2, c3} per Feistel round (padded)
     unsigned long long walk, rnd, shift, step;
     uint32_t slot, cand_next, abort, live;
     unsigned long long entry;  // resident launch: ring entry of the last trial
@@ -59,6 +59,8 @@ struct CtaShared {
     uint32_t slot_state[kMaxSlots];
     SlotHeader slot_hdr[kMaxSlots];
     uint32_t groups_done;
+    uint32_t next_class;  // fused launches: the class this CTA runs next
+    EngineArgs args;      // fused launches: the current class's arguments
 };
 static_assert(sizeof(CtaShared) <= kCtaSharedBytes, "the planner reserves kCtaSharedBytes");
 
@@ -139,6 +141,11 @@ __device__ __forceinline__ uint32_t find_job(const Job* jobs, uint32_t njobs, ui
     return lo;
 }
 
+__device__ __forceinline__ Round1 load_round1(const GroupHeader* gh, uint32_t r) {
+    const uint4 c4 = *reinterpret_cast<const uint4*>(&gh->r1[r][0]);
+    return Round1{c4.x, c4.z, c4.w, gh->r1[r][4], c4.y};
+}
+
 // Warp-aggregated claim of candidate indices from a shared counter.
 __device__ __forceinline__ uint32_t claim(uint32_t* counter, bool need, uint32_t lane) {
     const unsigned m = __ballot_sync(kFull, need);
@@ -174,8 +181,7 @@ __device__ __forceinline__ void build_map_direct(const Lanes& L, const Job& J, G
             uint32_t l = (uint32_t)left, r = (uint32_t)right;
 #pragma unroll 1
             for (uint32_t rr = 0; rr < 8; ++rr) {
-                const uint4 c4 = *reinterpret_cast<const uint4*>(&gh->r1[rr][0]);
-                const Round1 rc{c4.x, c4.y, c4.z, c4.w, gh->r1[rr][4]};
+                const Round1 rc = load_round1(gh, rr);
                 const uint32_t f = prp_f(L, key, rc, r) & (uint32_t)mask;
                 const uint32_t nr = (l ^ f) & (uint32_t)mask;
                 l = r;
@@ -285,35 +291,65 @@ __device__ __forceinline__ void map_from_cache(const Job& J, GroupHeader* gh, co
 }
 
 // Round cache: entry (r, R) = F_r(R) & mask for the 8 rounds and every h-bit
-// R, 8 * 2^h AES blocks.  Two independent blocks per iteration: their unrolled
-// round chains interleave, doubling the ILP of each warp.
-__device__ __forceinline__ void fill_round_cache(const Lanes& L, const PrpKey& key,
-                                                 const GroupHeader* gh, uint16_t* cache,
-                                                 uint32_t h, uint32_t m, uint32_t gt,
-                                                 uint32_t gthreads) {
+// R, 8 * 2^h AES blocks.  N independent blocks per iteration: their unrolled
+// round chains interleave, multiplying the ILP of each warp.  Rounds 1 and 2 come
+// from the group's fold table (prp_f_folded): cache entry e = (r << h) | R
+// uses fold entry (r << (h - 8)) | (R >> 8) = e >> 8 when h >= 8, and r =
+// e >> h below.  A warp covers 32 consecutive R of one round (entries start
+// 32-aligned), so its fold loads are one broadcast.
+template <int N>
+__device__ __forceinline__ void fill_round_cache_n(const Lanes& L, const PrpKey& key,
+                                                   const GroupHeader* gh, const uint4* fold,
+                                                   uint16_t* cache, uint32_t h, uint32_t m,
+                                                   uint32_t gt, uint32_t gthreads) {
     const uint32_t entries = 8u << h;
+    const uint32_t vsh = h > 8 ? 8 : h;
     uint32_t e = gt;
-    for (; e + gthreads < entries; e += 2 * gthreads) {
-        const uint32_t e2 = e + gthreads;
-        const uint32_t r1a = e >> h, r1b = e2 >> h;
-        const uint4 ca = *reinterpret_cast<const uint4*>(&gh->r1[r1a][0]);
-        const uint4 cb = *reinterpret_cast<const uint4*>(&gh->r1[r1b][0]);
-        const Round1 rca{ca.x, ca.y, ca.z, ca.w, gh->r1[r1a][4]};
-        const Round1 rcb{cb.x, cb.y, cb.z, cb.w, gh->r1[r1b][4]};
-        const uint32_t fa = prp_f(L, key, rca, e & m);
-        const uint32_t fb = prp_f(L, key, rcb, e2 & m);
-        cache[e] = (uint16_t)(fa & m);
-        cache[e2] = (uint16_t)(fb & m);
+    for (; e + (N - 1) * gthreads < entries; e += N * gthreads) {
+        uint32_t f[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const uint32_t ei = e + i * gthreads;
+            const uint2 k = *reinterpret_cast<const uint2*>(&gh->r1[ei >> h][0]);
+            f[i] = prp_f_folded(L, key, k.x, k.y, fold[ei >> vsh], ei & m);
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i) cache[e + i * gthreads] = (uint16_t)(f[i] & m);
     }
-    if (e < entries) {
-        const uint32_t rr = e >> h;
-        const uint4 c4 = *reinterpret_cast<const uint4*>(&gh->r1[rr][0]);
-        const Round1 rc{c4.x, c4.y, c4.z, c4.w, gh->r1[rr][4]};
-        cache[e] = (uint16_t)(prp_f(L, key, rc, e & m) & m);
+    for (; e < entries; e += gthreads) {
+        const uint2 k = *reinterpret_cast<const uint2*>(&gh->r1[e >> h][0]);
+        cache[e] = (uint16_t)(prp_f_folded(L, key, k.x, k.y, fold[e >> vsh], e & m) & m);
     }
 }
 
-template <typename MapT, typename BinT, bool WIDE, bool SPLIT>
+// n independent blocks per thread per step.  Only the kernels with walk slots
+// in shared memory carry the choice (default 3: config 2 measured 3.01 M
+// trials/s with 2, 3.03 M with 3, 3.02 M with 4); the global-slot kernels keep
+// a plain 2-block fill (cmc_engine below says why).
+template <bool VAR>
+__device__ __forceinline__ void fill_round_cache(const Lanes& L, const PrpKey& key,
+                                                 const GroupHeader* gh, const uint4* fold,
+                                                 uint16_t* cache, uint32_t h, uint32_t m,
+                                                 uint32_t gt, uint32_t gthreads, uint32_t n) {
+    if (VAR && n == 4) fill_round_cache_n<4>(L, key, gh, fold, cache, h, m, gt, gthreads);
+    else if (VAR && n != 2) fill_round_cache_n<3>(L, key, gh, fold, cache, h, m, gt, gthreads);
+    else fill_round_cache_n<2>(L, key, gh, fold, cache, h, m, gt, gthreads);
+}
+
+// The fold table of the group's current trial: entry v = (r, y) for Feistel
+// round r and y = R >> 8 (fold_entry in cmc_aes.cuh).
+__device__ __forceinline__ void build_fold_table(const Lanes& L, const PrpKey& key,
+                                                 const GroupHeader* gh, uint4* fold, uint32_t h,
+                                                 uint32_t gt, uint32_t gthreads) {
+    const uint32_t yb = h > 8 ? h - 8 : 0;
+    const uint32_t n = 8u << yb;
+    for (uint32_t v = gt; v < n; v += gthreads) {
+        const Round1 c = round1_consts(L, gh->rk, v >> yb, h);
+        fold[v] = fold_entry(L, key, c, v & ((1u << yb) - 1u));
+    }
+}
+
+template <typename MapT, typename BinT, bool WIDE, bool SPLIT, bool SMEMSLOTS>
 __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaShared* cs, uint32_t g,
                                          uint32_t gt) {
     const uint32_t gthreads = a.wg * 32;
@@ -321,7 +357,6 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
     const Lanes L{lane * 4, lane * 4 + 128, a.r256};
     char* gbase = smem + a.group_off + g * a.group_bytes;
     GroupHeader* gh = reinterpret_cast<GroupHeader*>(gbase);
-    uint16_t* cache = reinterpret_cast<uint16_t*>(gbase + sizeof(GroupHeader));
     uint32_t cursor = 0;
     const unsigned long long total = a.total_dev ? *a.total_dev : a.total;
 
@@ -460,12 +495,26 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         // the walker's last accesses to this slot happen-before ours
         if constexpr (SPLIT) __threadfence();
         else __threadfence_block();
+        // A job uses a round cache only if this launch provides room for it
+        // (a descriptor made under other options falls back to direct passes):
+        // its fold table, and a shared-memory cache after it.
+        const uint32_t cache_entries = 8u << J.half_bits;
+        const uint32_t fold_end = kGroupHeaderBytes + fold_table_bytes(J.half_bits);
+        const bool smem_cache = !WIDE && J.method == kMethodCache &&
+                                fold_end + 2 * cache_entries <= a.group_bytes;
+        const bool glob_cache = !WIDE && !smem_cache && J.method == kMethodGCache &&
+                                a.gcache != nullptr && cache_entries <= a.gcache_stride &&
+                                fold_end <= a.group_bytes;
+        uint4* fold = reinterpret_cast<uint4*>(gbase + kGroupHeaderBytes);
+        PrpKey key;
         if constexpr (!WIDE) {
+            prp_key_from_schedule(gh->rk, key);
             if (gt < 8) {
                 const Round1 c = round1_consts(L, gh->rk, gt, J.half_bits);
-                gh->r1[gt][0] = c.c0; gh->r1[gt][1] = c.c1; gh->r1[gt][2] = c.c2;
-                gh->r1[gt][3] = c.c3; gh->r1[gt][4] = c.w3hi;
+                gh->r1[gt][0] = c.c0; gh->r1[gt][1] = c.w3hi; gh->r1[gt][2] = c.c1;
+                gh->r1[gt][3] = c.c2; gh->r1[gt][4] = c.c3;
             }
+            if (smem_cache || glob_cache) build_fold_table(L, key, gh, fold, J.half_bits, gt, gthreads);
         }
         group_sync(g, gthreads);
 
@@ -480,20 +529,16 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
             uint4* b4 = reinterpret_cast<uint4*>(bins);
             for (uint32_t i = gt; i < nvec; i += gthreads) b4[i] = make_uint4(kFull, kFull, kFull, kFull);
         }
-        PrpKey key;
-        if constexpr (!WIDE) prp_key_from_schedule(gh->rk, key);
-        // A job uses a round cache only if this launch provides room for it
-        // (a descriptor made under other options falls back to direct passes).
-        const uint32_t cache_entries = 8u << J.half_bits;
-        if (!WIDE && J.method == kMethodCache &&
-            sizeof(GroupHeader) + 2 * cache_entries <= a.group_bytes) {
-            fill_round_cache(L, key, gh, cache, J.half_bits, (uint32_t)J.mask, gt, gthreads);
+        if (smem_cache) {
+            uint16_t* cache = reinterpret_cast<uint16_t*>(gbase + fold_end);
+            fill_round_cache<SMEMSLOTS>(L, key, gh, fold, cache, J.half_bits, (uint32_t)J.mask, gt,
+                                        gthreads, a.fill_blocks);
             group_sync(g, gthreads);
             map_from_cache<MapT>(J, gh, cache, map, lane, a.map_chains ? a.map_chains : 1);
-        } else if (!WIDE && J.method == kMethodGCache && a.gcache != nullptr &&
-                   cache_entries <= a.gcache_stride) {
+        } else if (glob_cache) {
             uint16_t* gc = a.gcache + (size_t)(blockIdx.x * a.ng + g) * a.gcache_stride;
-            fill_round_cache(L, key, gh, gc, J.half_bits, (uint32_t)J.mask, gt, gthreads);
+            fill_round_cache<SMEMSLOTS>(L, key, gh, fold, gc, J.half_bits, (uint32_t)J.mask, gt,
+                                        gthreads, a.fill_blocks);
             group_sync(g, gthreads);  // orders the group's global writes before its reads
             // four chains hide L2/DRAM latency unless cycle-walking is heavy
             // (c = 2^2h / D > 2), where idle chains' gathers cost more than
@@ -672,66 +717,69 @@ struct Walk {
         }
     }
 
-    // DRRT18 cycling eviction (cuckoo_core.hpp:134-158), one probe per step.
+    // DRRT18: one probe per step.
     __device__ __forceinline__ void drrt_steps(int n, unsigned long long& probes) {
 #pragma unroll 1
-        for (int s = 0; s < n && active; ++s) {
-            ++probes;
-            if (phase == 0) {
-                // a new item tries its copies in order
-                const uint32_t b = mem.map(item * k + choice);
-                if (out_of_range(b)) break;
-                if (mem.bin(b) == kEmpty) {
-                    mem.set(b, pack(item, choice));
-                    ++item;
-                    choice = 0;
-                    active = item != t;
-                } else if (++choice == k) {
-                    phase = 1;
-                    cur = item;
-                    choice = 0;
-                    target = mem.map(item * k);
-                    count = 0;
-                    if (out_of_range(target)) break;
-                }
-                continue;
-            }
-            const uint32_t displaced = mem.bin(target);
-            if (displaced == kEmpty) {
-                mem.set(target, pack(cur, choice));
+        for (int s = 0; s < n && active; ++s) drrt_step(probes);
+    }
+
+    // DRRT18 cycling eviction (cuckoo_core.hpp:134-158), one probe.
+    __device__ __forceinline__ void drrt_step(unsigned long long& probes) {
+        ++probes;
+        if (phase == 0) {
+            // a new item tries its copies in order
+            const uint32_t b = mem.map(item * k + choice);
+            if (out_of_range(b)) return;
+            if (mem.bin(b) == kEmpty) {
+                mem.set(b, pack(item, choice));
                 ++item;
-                phase = 0;
                 choice = 0;
                 active = item != t;
-                continue;
+            } else if (++choice == k) {
+                phase = 1;
+                cur = item;
+                choice = 0;
+                target = mem.map(item * k);
+                count = 0;
+                out_of_range(target);
             }
-            if (count >= kick) {
-                failed = true;
-                active = false;
-                break;
-            }
-            mem.set(target, pack(cur, choice));
-            cur = displaced & kOrdMask;
-            choice = (displaced >> kShift) & 3u;
-            const uint32_t previous = target;
-            bool found = false;
-            for (uint32_t j = 0; j < k; ++j) {
-                choice = choice + 1 == k ? 0 : choice + 1;
-                const uint32_t next = mem.map(cur * k + choice);
-                if (next != previous) {
-                    target = next;
-                    found = true;
-                    break;
-                }
-            }
-            if (!found) {
-                failed = true;
-                active = false;
-                break;
-            }
-            if (out_of_range(target)) break;
-            ++count;
+            return;
         }
+        const uint32_t displaced = mem.bin(target);
+        if (displaced == kEmpty) {
+            mem.set(target, pack(cur, choice));
+            ++item;
+            phase = 0;
+            choice = 0;
+            active = item != t;
+            return;
+        }
+        if (count >= kick) {
+            failed = true;
+            active = false;
+            return;
+        }
+        mem.set(target, pack(cur, choice));
+        cur = displaced & kOrdMask;
+        choice = (displaced >> kShift) & 3u;
+        const uint32_t previous = target;
+        bool found = false;
+        for (uint32_t j = 0; j < k; ++j) {
+            choice = choice + 1 == k ? 0 : choice + 1;
+            const uint32_t next = mem.map(cur * k + choice);
+            if (next != previous) {
+                target = next;
+                found = true;
+                break;
+            }
+        }
+        if (!found) {
+            failed = true;
+            active = false;
+            return;
+        }
+        if (out_of_range(target)) return;
+        ++count;
     }
 };
 
@@ -900,50 +948,25 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
     }
 }
 
-}  // namespace
-
-template <typename MapT, typename BinT, bool WIDE>
-__global__ void __launch_bounds__(512, 1) cmc_engine_split(const EngineArgs a) {
-    if (blockIdx.x >= a.producer_ctas) {
-        walker_split<MapT, BinT>(a);
-        return;
+// Bank-replicated table: row x = [T0[x] x 32][ror16(T0[x]) x 32].
+__device__ __forceinline__ void build_table(const uint32_t* t0, char* smem) {
+    uint32_t* tw = reinterpret_cast<uint32_t*>(smem);
+    for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) {
+        const uint32_t v = __ldg(&t0[i >> 6]);
+        tw[i] = (i & 32) ? __funnelshift_r(v, v, 16) : v;
     }
-    char* smem = cmc_dyn_smem;
-    {
-        uint32_t* tw = reinterpret_cast<uint32_t*>(smem);
-        for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) {
-            const uint32_t v = __ldg(&a.t0[i >> 6]);
-            tw[i] = (i & 32) ? __funnelshift_r(v, v, 16) : v;
-        }
-    }
-    __syncthreads();
-    const uint32_t warp = threadIdx.x >> 5;
-    if (warp < a.ng * a.wg)
-        producer<MapT, BinT, WIDE, true>(a, smem, nullptr, warp / a.wg,
-                                         threadIdx.x - (warp / a.wg) * a.wg * 32);
 }
 
-template <typename MapT, typename BinT, bool WIDE>
-__global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
-    char* smem = cmc_dyn_smem;
-    // Bank-replicated table: row x = [T0[x] x 32][ror16(T0[x]) x 32].
-    {
-        uint32_t* tw = reinterpret_cast<uint32_t*>(smem);
-        for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) {
-            const uint32_t v = __ldg(&a.t0[i >> 6]);
-            tw[i] = (i & 32) ? __funnelshift_r(v, v, 16) : v;
-        }
-    }
-    CtaShared* cs = reinterpret_cast<CtaShared*>(smem + kCtaSharedOff);
-    for (uint32_t i = threadIdx.x; i < kMaxSlots; i += blockDim.x) cs->slot_state[i] = kSlotFree;
-    if (threadIdx.x == 0) cs->groups_done = 0;
-    __syncthreads();
-    // Warp roles.  Warp w issues from SM sub-partition w % 4.  With
-    // isolate_walkers the nw walker warps take ids 15, 11, 7, 3 (all on
-    // sub-partition 3) and producers take sub-partitions 0..2 first (12
-    // warps), then the sub-partition-3 ids no walker uses.  The latency-bound
-    // walks then share their issue slots with few or no throughput-bound AES
-    // warps.
+// Warp roles of one engine run over `a` (the caller has built the table and
+// cleared the CTA's slot states).  Warp w issues from SM sub-partition w % 4.
+// With isolate_walkers the nw walker warps take ids 15, 11, 7, 3 (all on
+// sub-partition 3) and producers take sub-partitions 0..2 first (12 warps),
+// then the sub-partition-3 ids no walker uses.  The latency-bound walks then
+// share their issue slots with few or no throughput-bound AES warps.  Warps
+// with no role return at once.  SMEMSLOTS: the plan keeps its walk slots in
+// shared memory (a.gslots null) or, if false, in global memory.
+template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
+__device__ __forceinline__ void engine_roles(const EngineArgs& a, char* smem, CtaShared* cs) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t producer_idx = 0xffffffffu, walker_idx = 0xffffffffu;
     if (a.isolate_walkers) {
@@ -957,10 +980,97 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
     }
     if (producer_idx < a.ng * a.wg) {
         const uint32_t g = producer_idx / a.wg;
-        producer<MapT, BinT, WIDE, false>(a, smem, cs, g, (producer_idx % a.wg) * 32 + lane);
+        producer<MapT, BinT, WIDE, false, SMEMSLOTS>(a, smem, cs, g, (producer_idx % a.wg) * 32 + lane);
     } else if (walker_idx < a.nw) {
-        if (a.gslots) walker<MapT, BinT, false>(a, cs, walker_idx);
-        else walker<MapT, BinT, true>(a, cs, walker_idx);
+        walker<MapT, BinT, SMEMSLOTS>(a, cs, walker_idx);
+    }
+}
+
+__device__ __forceinline__ void reset_cta_slots(CtaShared* cs) {
+    for (uint32_t i = threadIdx.x; i < kMaxSlots; i += blockDim.x) cs->slot_state[i] = kSlotFree;
+    if (threadIdx.x == 0) cs->groups_done = 0;
+}
+
+}  // namespace
+
+template <typename MapT, typename BinT, bool WIDE>
+__global__ void __launch_bounds__(512, 1) cmc_engine_split(const EngineArgs a) {
+    if (blockIdx.x >= a.producer_ctas) {
+        walker_split<MapT, BinT>(a);
+        return;
+    }
+    char* smem = cmc_dyn_smem;
+    build_table(a.t0, smem);
+    __syncthreads();
+    const uint32_t warp = threadIdx.x >> 5;
+    if (warp < a.ng * a.wg)
+        producer<MapT, BinT, WIDE, true, false>(a, smem, nullptr, warp / a.wg,
+                                         threadIdx.x - (warp / a.wg) * a.wg * 32);
+}
+
+// One instantiation per entry width and walk-slot placement.  The walkers'
+// loop over global slots (two dependent L2/DRAM round trips per probe) turned
+// ~4.4x slower when anything changed the register allocation of the kernel
+// around it -- a 3- and 4-block variant of the round-cache fill, one more
+// value held in the walker (measured, on B200; round trips per warp step
+// 5.2k -> 23k cycles) -- so the global-slot kernels are compiled without those
+// and the shared-slot kernels, whose walks are unaffected, keep the
+// fill_blocks choice.
+template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
+__global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
+    char* smem = cmc_dyn_smem;
+    build_table(a.t0, smem);
+    CtaShared* cs = reinterpret_cast<CtaShared*>(smem + kCtaSharedOff);
+    reset_cta_slots(cs);
+    __syncthreads();
+    engine_roles<MapT, BinT, WIDE, SMEMSLOTS>(a, smem, cs);
+}
+
+// Plan classes of a batched call in one launch (FusedArgs in cmc_engine.cuh),
+// all of one entry width and walk-slot placement.  A class's run ends for a
+// CTA when its producers find no trial left to claim and its walker has walked
+// every filled slot; the CTA then picks its next class.  The table is built
+// once.
+template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
+__global__ void __launch_bounds__(512, 1) cmc_engine_fused(const __grid_constant__ FusedArgs f) {
+    char* smem = cmc_dyn_smem;
+    build_table(f.cls[0].t0, smem);
+    CtaShared* cs = reinterpret_cast<CtaShared*>(smem + kCtaSharedOff);
+    uint32_t c = 0;
+    while (c + 1 < f.nclass && blockIdx.x >= f.first_cta[c + 1]) ++c;
+    for (;;) {
+        // the class's arguments, copied to shared memory: the roles read them
+        // at shared-memory latency rather than through generic loads of the
+        // parameter block
+        reset_cta_slots(cs);
+        {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(&f.cls[c]);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&cs->args);
+            for (uint32_t i = threadIdx.x; i < sizeof(EngineArgs) / 4; i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        engine_roles<MapT, BinT, WIDE, SMEMSLOTS>(cs->args, smem, cs);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // the class with the most estimated work left; none: this CTA is done
+            uint32_t best = 0xffffffffu;
+            float best_left = 0.0f;
+            for (uint32_t k = 0; k < f.nclass; ++k) {
+                const EngineArgs& b = f.cls[k];
+                const unsigned long long claimed = atomicAdd(&b.ctrl->next, 0ULL);
+                const unsigned long long size = b.total - b.gidx_begin;
+                if (atomicAdd(&b.ctrl->error, 0u) || claimed >= size) continue;
+                const float left = float(size - claimed) * f.cost[k];
+                if (left > best_left) {
+                    best_left = left;
+                    best = k;
+                }
+            }
+            cs->next_class = best;
+        }
+        __syncthreads();
+        c = cs->next_class;
+        if (c >= f.nclass) break;
     }
 }
 
@@ -1012,8 +1122,8 @@ __global__ void __launch_bounds__(1024) cmc_compact_failures(const uint32_t* __r
 }
 
 // Device self-test: the FIPS-197 AES-128 vector on every lane through the
-// shared-memory table, and the 124-lookup PRP round function against the
-// full encryption for pseudo-random keys, rounds and inputs.
+// shared-memory table, and the 124-lookup PRP round function and its folded
+// form against the full encryption for pseudo-random keys, rounds and inputs.
 __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32_t* out,
                              uint32_t r256) {
     char* smem = cmc_dyn_smem;
@@ -1049,17 +1159,29 @@ __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32
         uint32_t full[4];
         encrypt_full(L, rk, 0x43455350u, r, h, R, full);
         if ((prp_f(L, key, rc, R) & 0xffffu) != (full[3] & 0xffffu)) bad |= 4;
+        // the round-2 fold of the round-cache fill gives the same value
+        const uint4 v = fold_entry(L, key, rc, R >> 8);
+        if ((prp_f_folded(L, key, rc.c0, rc.w3hi, v, R) & 0xffffu) != (full[3] & 0xffffu)) bad |= 8;
 
     }
     out[threadIdx.x] = bad;
 }
 
 // Explicit instantiations used by the launcher.
-template __global__ void cmc_engine<uint16_t, uint16_t, false>(const EngineArgs);
-template __global__ void cmc_engine<uint32_t, uint32_t, false>(const EngineArgs);
-template __global__ void cmc_engine<uint32_t, uint32_t, true>(const EngineArgs);
+template __global__ void cmc_engine<uint16_t, uint16_t, false, true>(const EngineArgs);
+template __global__ void cmc_engine<uint32_t, uint32_t, false, true>(const EngineArgs);
+template __global__ void cmc_engine<uint32_t, uint32_t, true, true>(const EngineArgs);
+template __global__ void cmc_engine<uint16_t, uint16_t, false, false>(const EngineArgs);
+template __global__ void cmc_engine<uint32_t, uint32_t, false, false>(const EngineArgs);
+template __global__ void cmc_engine<uint32_t, uint32_t, true, false>(const EngineArgs);
 template __global__ void cmc_engine_split<uint16_t, uint16_t, false>(const EngineArgs);
 template __global__ void cmc_engine_split<uint32_t, uint32_t, false>(const EngineArgs);
 template __global__ void cmc_engine_split<uint32_t, uint32_t, true>(const EngineArgs);
+template __global__ void cmc_engine_fused<uint16_t, uint16_t, false, true>(const __grid_constant__ FusedArgs);
+template __global__ void cmc_engine_fused<uint32_t, uint32_t, false, true>(const __grid_constant__ FusedArgs);
+template __global__ void cmc_engine_fused<uint32_t, uint32_t, true, true>(const __grid_constant__ FusedArgs);
+template __global__ void cmc_engine_fused<uint16_t, uint16_t, false, false>(const __grid_constant__ FusedArgs);
+template __global__ void cmc_engine_fused<uint32_t, uint32_t, false, false>(const __grid_constant__ FusedArgs);
+template __global__ void cmc_engine_fused<uint32_t, uint32_t, true, false>(const __grid_constant__ FusedArgs);
 
 }  // namespace cmc

@@ -19,6 +19,13 @@ constexpr uint32_t kEngineTableBytes = 65536;  // replicated T-table at shared o
 constexpr uint32_t kMaxGroups = 14; // named barriers 1..14
 constexpr uint32_t kGroupHeaderBytes = 1024;  // per-group shared header (the trial's job copy)
 
+// A group's shared region: [header, kGroupHeaderBytes][round-2 fold table of a
+// round-cache job][the round cache itself, when it is kept in shared memory].
+// The fold table holds 8 rounds x 2^max(0, h - 8) entries of 16 bytes.
+__host__ __device__ constexpr uint32_t fold_table_bytes(uint32_t h) {
+    return 16u * (8u << (h > 8 ? h - 8 : 0));
+}
+
 // One experiment configuration applied to a contiguous run of trials of one
 // batch.  The job table concatenates its jobs' trials: job j owns global
 // indices [trial_base, trial_base + count); a launch runs a contiguous range.
@@ -88,7 +95,7 @@ struct EngineArgs {
     // Job::user (the server slot) rather than by table position
     const unsigned long long* total_dev;
     uint32_t count_by_user;
-    uint32_t group_bytes;               // per-group smem (header + cache)
+    uint32_t group_bytes;               // per-group smem (header + fold table + cache)
     uint32_t group_off;                 // smem offset of group 0
     uint32_t slots_off;                 // smem offset of slot 0 (smem slots)
     uint32_t spin_limit;                // producer waits: microseconds before one gives up
@@ -105,10 +112,27 @@ struct EngineArgs {
     const ResidentQueue* rq;
     uint32_t ring_mask;
     uint32_t map_chains;                // lookup chains per lane from a round cache (0: automatic)
+    uint32_t fill_blocks;               // round-cache fill: blocks per thread per step (0: automatic)
     unsigned long long entry_begin;
     unsigned long long bits_mask;
     unsigned int* entry_done;
 };
+
+// Batched calls: ONE persistent launch over the plan classes of a call (all
+// classes of one entry width; see cmc_engine_fused).  Each
+// class keeps its own engine arguments (plan, job range, control block and
+// global pool region); CTAs [first_cta[c], first_cta[c + 1]) start on class c
+// (in proportion to its estimated work), and a CTA whose class has no trials
+// left to claim moves on to the class with the most estimated work left
+// (unclaimed trials x cost per trial).
+constexpr uint32_t kMaxFusedClasses = 16;
+struct FusedArgs {
+    EngineArgs cls[kMaxFusedClasses];
+    float cost[kMaxFusedClasses];            // estimated AES blocks per trial
+    uint16_t first_cta[kMaxFusedClasses + 1];
+    uint32_t nclass;
+};
+static_assert(sizeof(FusedArgs) <= 4096, "fused launch arguments fit the classic parameter space");
 
 // Serving: device-resident state of one admitted job.  `next` is the job's
 // RNG counter -- the index of its next trial in the experiment, whose batch

@@ -34,8 +34,6 @@
 
 namespace cmc {
 
-template <typename MapT, typename BinT, bool WIDE>
-__global__ void cmc_engine(const EngineArgs a);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
                                      uint32_t* out, uint32_t* count, uint64_t cap,
                                      const unsigned long long* nbits_dev);
@@ -206,9 +204,7 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
     a.slots_off = pl.slots_off;
     a.spin_limit = pl_ctx.spin_limit;
     a.idle_polls = pl_ctx.spin_limit;
-    const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
-                   : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
-                                     : (const void*)cmc_engine<uint32_t, uint32_t, true>;
+    const void* fn = engine_kernel(pl.variant, true);  // walk slots in shared memory (checked above)
     // the engine's shared-memory limit was raised to the device maximum at set-up
     void* args[] = {&a};
     e = cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, s);

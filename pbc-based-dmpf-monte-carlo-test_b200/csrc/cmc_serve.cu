@@ -46,8 +46,6 @@
 
 namespace cmc {
 
-template <typename MapT, typename BinT, bool WIDE>
-__global__ void cmc_engine(const EngineArgs a);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
                                      uint32_t* out, uint32_t* count, uint64_t cap,
                                      const unsigned long long* nbits_dev);
@@ -658,9 +656,8 @@ struct Server {
         a.spin_limit = ctx->spin_limit;
         a.idle_polls = ctx->spin_limit;
         a.map_chains = ctx->map_chains;
-        const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
-                       : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
-                                         : (const void*)cmc_engine<uint32_t, uint32_t, true>;
+        a.fill_blocks = ctx->fill_blocks;
+        const void* fn = engine_kernel(pl.variant, pl.slots_smem);
         // the context raised the engine's shared-memory limit to the device maximum
         void* args[] = {&a};
         if ((rc = cuda(cudaEventRecord(b.e0, st), "event"))) return rc;
@@ -982,9 +979,8 @@ struct Server {
         a.slots_off = pl.slots_off;
         a.spin_limit = ctx->spin_limit;
         a.map_chains = ctx->map_chains;
-        const void* fn = pl.variant == 0 ? (const void*)cmc_engine<uint16_t, uint16_t, false>
-                       : pl.variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false>
-                                         : (const void*)cmc_engine<uint32_t, uint32_t, true>;
+        a.fill_blocks = ctx->fill_blocks;
+        const void* fn = engine_kernel(pl.variant, pl.slots_smem);
         // the context raised the engine's shared-memory limit to the device maximum
         void* args[] = {&a};
         if ((rc = cuda(cudaEventRecord(r_e0, st), "event"))) return rc;

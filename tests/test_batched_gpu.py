@@ -51,18 +51,65 @@ def test_capacity_limits_offsets_not_counts(ctx, cmc):
     assert failed[0] == len(full)
 
 
-def test_plan_classes(ctx, cmc):
-    # long-walk sets (global walk slots) and short ones (shared-memory slots)
-    # run as separate launches of one call, each under its own plan
-    jobs = [(cmc.parameters("bgh25", 8000, 24, 3, 11200, 500, "affine"), 5, 0, 0, 96),
+def plan_class_jobs(cmc):
+    # long-walk sets (global walk slots) and short ones (shared-memory slots):
+    # several plan classes of one entry width
+    return [(cmc.parameters("bgh25", 8000, 24, 3, 11200, 500, "affine"), 5, 0, 0, 96),
             (cmc.parameters("bgh25", 64, 16, 3, 80, 50, "affine"), 11, 1, 10, 3000),
             (cmc.parameters("drrt18", 3000, 24, 2, 3600, 100, "affine"), 6, 2, 0, 64),
             (cmc.parameters("bgh25", 300, 20, 4, 340, 100, "sequential"), 7, 0, 5, 700)]
-    failed, per_job = ctx.run_jobs(jobs)
-    assert " | " in ctx.last_plan and ctx.last_kernel_count >= 3
+
+
+@pytest.mark.parametrize("fused", [1, 0])
+def test_plan_classes(ctx, cmc, fused):
+    # each class runs under its own plan: all of them in one persistent launch
+    # (fused, the default) or one launch per class
+    jobs = plan_class_jobs(cmc)
+    ctx.set_option("fused", fused)
+    try:
+        failed, per_job = ctx.run_jobs(jobs)
+    finally:
+        ctx.set_option("fused", 1)
+    assert " | " in ctx.last_plan
+    if fused:
+        # classes of one entry width and walk-slot placement share a launch:
+        # here shared-slot and global-slot classes, two launches + compaction
+        assert ctx.last_plan.startswith("fused(") and ctx.last_kernel_count == 3
+    else:
+        assert ctx.last_kernel_count == 5
     for i, (p, s, b, first, count) in enumerate(jobs):
         assert per_job[i] == ctx.launch(p, cmc.batch_key(s, b), first, count), i
         assert failed[i] == len(per_job[i])
+
+
+def test_fused_with_other_entry_width(ctx, cmc):
+    # a class with 32-bit entries (B > 65535) runs in a launch of its own
+    # beside the fused launch of the 16-bit shared-slot classes (t = 64 and
+    # t = 300); the 16-bit global-slot class (t = 3000) is alone in its kind
+    # and runs by itself too; every job as alone
+    jobs = plan_class_jobs(cmc)[1:] + [
+        (cmc.parameters("bgh25", 50000, 20, 3, 70000, 50, "affine"), 9, 0, 0, 8)]
+    failed, per_job = ctx.run_jobs(jobs)
+    assert ctx.last_plan.startswith("fused(") and ctx.last_kernel_count == 4
+    for i, (p, s, b, first, count) in enumerate(jobs):
+        assert per_job[i] == ctx.launch(p, cmc.batch_key(s, b), first, count), i
+
+
+def test_fused_uneven_classes_share_ctas(ctx, cmc):
+    # one heavy class and many light ones: CTAs that finish a light class move
+    # to the heavy one; the result equals the launches one class at a time
+    jobs = [(cmc.parameters("bgh25", 2500, 24, 3, 3300, 300, "affine"), 21, 0, 0, 600),
+            (cmc.parameters("bgh25", 40, 16, 3, 50, 20, "affine"), 22, 0, 0, 20000),
+            (cmc.parameters("bgh25", 200, 20, 2, 260, 60, "affine"), 23, 3, 7, 5000)]
+    want = ctx.run_jobs(jobs)
+    plan = ctx.last_plan
+    ctx.set_option("fused", 0)
+    try:
+        assert ctx.run_jobs(jobs) == want
+    finally:
+        ctx.set_option("fused", 1)
+    if " | " in plan:
+        assert plan.startswith("fused(")
 
 
 def test_graph_capture_and_replay(ctx, cmc):
