@@ -12,7 +12,7 @@
 // One AES round column with T1 = ror8(T0) and T3 = ror8(T2):
 //   t = T0[a] ^ T2[c] ^ ror8(T0[b] ^ T2[d] ^ rol8(k))
 // so the round key is stored pre-rotated (rol8) and each column costs
-// 4 PRMT + 4 LDS + 2 LOP3 + 1 rotate.
+// 4 PRMT + 4 LDS + 2 LOP3 + 1 rotate (a fifth PRMT).
 //
 // The PRP round function of the reference (cuckoo_bench.cu:161-184) is
 //   F_r(R) = AES_k(0x43455350, r, h, R).w3 & (2^h - 1)
@@ -35,8 +35,18 @@ constexpr uint32_t kTableBytes = 65536;
 #define CMC_FMA_OFFSETS 0
 #endif
 
-__device__ __forceinline__ uint32_t ror8(uint32_t x) { return __funnelshift_r(x, x, 8); }
-__device__ __forceinline__ uint32_t rol8(uint32_t x) { return __funnelshift_l(x, x, 8); }
+// Rotations by one byte as byte permutes, and the column's two three-way XORs
+// as explicit three-input logic operations (0x96 = a ^ b ^ c): measured on
+// B200 at config 2, 3.071 M trials/s against 3.034 M with funnel shifts and
+// plain XORs.
+__device__ __forceinline__ uint32_t ror8(uint32_t x) { return __byte_perm(x, x, 0x0321); }
+__device__ __forceinline__ uint32_t rol8(uint32_t x) { return __byte_perm(x, x, 0x2103); }
+
+__device__ __forceinline__ uint32_t xor3(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t d;
+    asm("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
 
 // Byte offset of this lane's T0 (lb = lane*4) or T2 (lb = lane*4 + 128) entry
 // for byte `B` of word w.
@@ -80,7 +90,7 @@ __device__ __forceinline__ uint32_t column(const Lanes& L, uint32_t sa, uint32_t
     const uint32_t b = lds(toff<2>(sb, L.lb0));
     const uint32_t c = lds(toff<1>(sc, L.lb2));
     const uint32_t d = lds(toff<0>(sd, L.lb2));
-    return a ^ c ^ ror8(b ^ d ^ kr);
+    return xor3(a, c, ror8(xor3(b, d, kr)));
 }
 
 __device__ __forceinline__ uint32_t sbox_byte(const Lanes& L, uint32_t x) {
