@@ -681,9 +681,9 @@ int Ctx::prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::v
         batch_key(in[i].seed, in[i].batch, tmp[i].batch_rk);
         tmp[i].user = i;
     }
-    // Plan classes: parameter sets whose own plans agree (slot placement and
-    // count, warps per group, groups, walkers, entry width, cache kind) run
-    // under one plan, so a small table never runs under
+    // Plan classes: parameter sets whose own plans agree (slot placement,
+    // warps per group, groups, walkers, entry width, cache kind) run under one
+    // plan, so a small table never runs under
     // a plan made for a large one.  Classes run heaviest first; within a class, heaviest
     // trials first, so a launch ends on short ones.  Past kMaxClasses
     // signatures the lightest classes share the last launch.
@@ -697,12 +697,12 @@ int Ctx::prepare_jobs(const cmc_job* in, uint32_t n, uint32_t sample_div, std::v
             int rc = plan(std::vector<Job>{tmp[i]}, solo);
             if (rc) return rc;
             const char cache = tmp[i].method == kMethodCache ? 's' : tmp[i].method == kMethodGCache ? 'g' : 'd';
-            // the slot count too: a class's plan is sized for its largest
-            // table, so a small table in a class of large ones would walk in
-            // fewer slots than its own plan gives it
-            char key[128];
-            snprintf(key, sizeof key, "%d/%u/%u/%u/%u/%d/%c/%u", solo.slots_smem ? 1 : 0, solo.wg,
-                     solo.ng, solo.nw, solo.isolate, solo.variant, cache, solo.ns);
+            // (splitting classes further, by slot count, measured slower: 12
+            // classes on the 64-set sweep gave 1.069 M trials/s against 1.090 M
+            // with these 5 -- each class a CTA leaves costs it a walk drain)
+            char key[96];
+            snprintf(key, sizeof key, "%d/%u/%u/%u/%u/%d/%c", solo.slots_smem ? 1 : 0, solo.wg, solo.ng,
+                     solo.nw, solo.isolate, solo.variant, cache);
             auto it = ids.emplace(key, uint32_t(ids.size())).first;
             sig[i] = it->second;
             if (weight.size() <= sig[i]) weight.resize(sig[i] + 1, 0.0);
