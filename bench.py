@@ -385,6 +385,63 @@ def run_reference_gpu_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------- other single-set workloads --
+
+def workload_summary(cmc, ctx, w: dict, sms: int, max_mhz: float, steps: int = 4,
+                     warmup: int = 3) -> dict:
+    """A compact line for another single-configuration workload, measured after
+    the main timed region: device-resident launches over batches warmup..,
+    timed with CUDA events (L2 flushed between steps), the roofline fraction,
+    e2e through cmc_launch with host buffers, and a bounded CPU sample of the
+    reference's own code with its failure list compared on the GPU."""
+    import torch
+    p = cmc.parameters(w["mode"], w["pnum"], w["ell_i"], w["k"], w["buckets"], w["kick"],
+                       w["input_mode"])
+    n = min(w["trials"], 1 << w["bt"])
+    stream = torch.cuda.Stream()
+    d_out = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_n = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    keys = [torch.tensor(cmc.batch_key(w["seed"], b), dtype=torch.int64).to(torch.int32).cuda()
+            for b in range(warmup + steps)]
+    for b in range(warmup):
+        ctx.launch_device(p, keys[b].data_ptr(), 0, n, d_out.data_ptr(), d_n.data_ptr(),
+                          stream.cuda_stream)
+    torch.cuda.synchronize()
+    ctx.check()
+    total_ms, engine_ms = 0.0, []
+    for b in range(warmup, warmup + steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.launch_device(p, keys[b].data_ptr(), 0, n, d_out.data_ptr(), d_n.data_ptr(),
+                          stream.cuda_stream)
+        e1.record(stream)
+        engine_ms.append(ctx.last_engine_ms())
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    ctx.check()
+    value = n * steps / (total_ms / 1e3)
+    host_keys = [cmc.batch_key(w["seed"], warmup + steps + b) for b in range(2)]
+    ctx.launch(p, host_keys[0], 0, n)
+    t0 = time.perf_counter()
+    ctx.launch(p, host_keys[1], 0, n)
+    e2e = n / (time.perf_counter() - t0)
+    blocks = algorithmic_blocks(p)
+    achieved = blocks * AES_BYTES_PER_BLOCK * n / (statistics.mean(engine_ms) / 1e3) / 1e9
+    peak = sms * SMEM_BYTES_PER_CLK_PER_SM * max_mhz * 1e6 / 1e9
+    base, n_cpu, cpu_fails = cpu_baseline(5.0, w)
+    return {"workload": w["workload"], "value": value, "unit": "trials/s",
+            "steps": steps, "warmup": warmup, "ms_per_step": total_ms / steps,
+            "e2e": {"value": e2e, "unit": "trials/s",
+                    "timing": "host wall clock around one cmc_launch with host buffers"},
+            "roofline": {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak},
+            "plan": ctx.last_plan, "cpu_baseline": base,
+            "parity": parity_check(ctx, cmc, w, n_cpu, cpu_fails, base["kind"])}
+
+
 # ------------------------------------------------------------ sweep workload --
 
 def sweep_sets(n_sets: int = 64, draw_seed: int = 3):
@@ -771,7 +828,9 @@ def main():
         if world == 1 and args.workload == "config2" and not args.no_extras:
             # the batching and serving patterns, measured on the same box after
             # the timed region (own contexts; bounded to about a minute each)
-            for name, fn in (("sweep", lambda c: sweep_measure(cmc, c, args.sweep_trials)),
+            for name, fn in (("config1", lambda c: workload_summary(cmc, c, WORKLOADS["config1"], sms, max_mhz)),
+                             ("config4", lambda c: workload_summary(cmc, c, WORKLOADS["config4"], sms, max_mhz)),
+                             ("sweep", lambda c: sweep_measure(cmc, c, args.sweep_trials)),
                              ("serve", lambda c: serve_measure(cmc, c, args))):
                 c2 = cmc.Context(local)
                 try:
