@@ -230,8 +230,9 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
  * The first call on a device sets up that device (symbol addresses, a 1 KiB
  * table upload), so it should come before any stream capture.  All calls on a
  * device share the working memory: calls that overlap on the GPU race, so order
- * them (e.g. one stream).  If a bounded device wait gives up, *d_out_nfailed is
- * set to 0xffffffff.  Errors: cmc_last_error(NULL). */
+ * them (e.g. one stream).  If a bounded device wait gives up or a device-side
+ * check fails, *d_out_nfailed is set to 0xffffffff.  Errors:
+ * cmc_last_error(NULL). */
 int cmc_launch_static(const cmc_params* params, const uint32_t* d_batch_key, uint32_t first,
                       uint32_t count, uint32_t* d_out_offsets, uint32_t* d_out_nfailed,
                       void* stream);

@@ -37,8 +37,8 @@ constexpr uint32_t kTableBytes = 65536;
 
 // Rotations by one byte as byte permutes, and the column's two three-way XORs
 // as explicit three-input logic operations (0x96 = a ^ b ^ c): measured on
-// B200 at config 2, 3.071 M trials/s against 3.034 M with funnel shifts and
-// plain XORs.
+// B200 at t = 1024, B = 1536, N = 2^20: 3.071 M trials/s against 3.034 M
+// with funnel shifts and plain XORs.
 __device__ __forceinline__ uint32_t ror8(uint32_t x) { return __byte_perm(x, x, 0x0321); }
 __device__ __forceinline__ uint32_t rol8(uint32_t x) { return __byte_perm(x, x, 0x2103); }
 
@@ -55,13 +55,35 @@ __device__ __forceinline__ uint32_t toff(uint32_t w, uint32_t lb) {
     return __byte_perm(w, lb, 0x5504 | (B << 4));
 }
 
-// The table sits at offset 0 of dynamic shared memory.  Indexing the
-// extern __shared__ symbol itself keeps every lookup a shared-space load
-// whose symbol offset folds into the instruction's immediate.
+// The table sits at offset 0 of dynamic shared memory.
 extern __shared__ __align__(1024) char cmc_dyn_smem[];
 
+// Shared-window address at which dynamic shared memory starts in a kernel
+// with no static shared variables: after the 1 KiB the hardware reserves per
+// block on sm_90 and later (cudaDevAttrReservedSharedMemoryPerBlock).
+#define CMC_DYN_SMEM_BASE 1024
+#define CMC_STR_(x) #x
+#define CMC_STR(x) CMC_STR_(x)
+constexpr uint32_t kDynSmemBase = CMC_DYN_SMEM_BASE;
+
+// Every kernel that calls lds() checks this once (cmc_selftest at context
+// creation, the engine kernels at entry) and reports an error instead of
+// reading the table at a wrong address.
+__device__ __forceinline__ bool table_base_ok() {
+    return (uint32_t)__cvta_generic_to_shared(cmc_dyn_smem) == kDynSmemBase;
+}
+
+// One table lookup: a shared load at [off + base] with the base as the
+// instruction's immediate.  Written as a C++ load from cmc_dyn_smem + off, the
+// compiler kept the base in a register in the engine kernels and spent one
+// more (FMA-pipe) instruction per lookup on the add (measured on B200 at
+// t = 1024, B = 1536, N = 2^20: 517 against 404 instructions per 32 blocks,
+// 140 against 27 on the FMA pipe; 3.07 M against 3.35 M trials/s).  volatile keeps every lookup
+// after the barrier that publishes the table.
 __device__ __forceinline__ uint32_t lds(uint32_t off) {
-    return *reinterpret_cast<const uint32_t*>(cmc_dyn_smem + off);
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1+" CMC_STR(CMC_DYN_SMEM_BASE) "];" : "=r"(v) : "r"(off));
+    return v;
 }
 
 struct Lanes {

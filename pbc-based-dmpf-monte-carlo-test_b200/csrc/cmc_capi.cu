@@ -455,7 +455,8 @@ int Ctx::check_ctrl() {
     }
     last_ctrl = sum;
     if (sum.error)
-        return fail(-int(sum.error), "device wait gave up (site %u): results discarded", sum.where);
+        return fail(-int(sum.error), "%s (site %u): results discarded", ctrl_error_text(sum.error),
+                    sum.where);
     return CMC_OK;
 }
 

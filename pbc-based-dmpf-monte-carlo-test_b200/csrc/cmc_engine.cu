@@ -34,6 +34,7 @@ namespace cmc {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kErrBase = 3;     // == -CMC_EKAT: table_base_ok() failed
 constexpr uint32_t kErrTimeout = 4;  // == -CMC_ETIMEOUT
 constexpr uint32_t kErrRange = 5;    // == -CMC_ERANGE
 
@@ -108,6 +109,34 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 
 __device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// 16-bit stores of the round cache fill, written as PTX.  As plain C++
+// stores into the array that also holds the T-table, they cost one extra
+// FMA-pipe instruction per table lookup of the loop (measured on B200 with a
+// copy of the fill loop: 433 against 321 instructions per 32 blocks, 116
+// against 4 on the FMA pipe; the producers' issue slots are the limit).  The
+// memory clobber keeps them ordered with the other memory accesses.
+__device__ __forceinline__ void st_shared_u16(uint16_t* p, uint32_t v) {
+    asm volatile("st.shared.u16 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)),
+                 "h"((unsigned short)v)
+                 : "memory");
+}
+
+__device__ __forceinline__ void st_global_u16(uint16_t* p, uint32_t v) {
+    asm volatile("st.global.u16 [%0], %1;" ::"l"(__cvta_generic_to_global(p)),
+                 "h"((unsigned short)v)
+                 : "memory");
+}
+
+// Map entries of the direct pass, written the same way (the slot holding the
+// map sits in shared or global memory: a generic store).
+__device__ __forceinline__ void st_map(uint16_t* p, uint32_t v) {
+    asm volatile("st.u16 [%0], %1;" ::"l"(p), "h"((unsigned short)v) : "memory");
+}
+
+__device__ __forceinline__ void st_map(uint32_t* p, uint32_t v) {
+    asm volatile("st.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 __device__ __forceinline__ void group_sync(uint32_t g, uint32_t nthreads) {
@@ -204,7 +233,7 @@ __device__ __forceinline__ void build_map_direct(const Lanes& L, const Job& J, G
             uint32_t b;
             if constexpr (!WIDE) b = div_width((uint32_t)y, (uint32_t)J.width, J.width_magic);
             else b = (uint32_t)(y / J.width);
-            map[c] = (MapT)b;
+            st_map(map + c, b);
         } else if (has) {
             left = y >> h;
             right = y & mask;
@@ -297,11 +326,15 @@ __device__ __forceinline__ void map_from_cache(const Job& J, GroupHeader* gh, co
 // uses fold entry (r << (h - 8)) | (R >> 8) = e >> 8 when h >= 8, and r =
 // e >> h below.  A warp covers 32 consecutive R of one round (entries start
 // 32-aligned), so its fold loads are one broadcast.
-template <int N>
+template <int N, bool SHARED>
 __device__ __forceinline__ void fill_round_cache_n(const Lanes& L, const PrpKey& key,
                                                    const GroupHeader* gh, const uint4* fold,
                                                    uint16_t* cache, uint32_t h, uint32_t m,
                                                    uint32_t gt, uint32_t gthreads) {
+    auto put = [&](uint32_t i, uint32_t v) {
+        if constexpr (SHARED) st_shared_u16(cache + i, v);
+        else st_global_u16(cache + i, v);
+    };
     const uint32_t entries = 8u << h;
     const uint32_t vsh = h > 8 ? 8 : h;
     uint32_t e = gt;
@@ -314,26 +347,26 @@ __device__ __forceinline__ void fill_round_cache_n(const Lanes& L, const PrpKey&
             f[i] = prp_f_folded(L, key, k.x, k.y, fold[ei >> vsh], ei & m);
         }
 #pragma unroll
-        for (int i = 0; i < N; ++i) cache[e + i * gthreads] = (uint16_t)(f[i] & m);
+        for (int i = 0; i < N; ++i) put(e + i * gthreads, f[i] & m);
     }
     for (; e < entries; e += gthreads) {
         const uint2 k = *reinterpret_cast<const uint2*>(&gh->r1[e >> h][0]);
-        cache[e] = (uint16_t)(prp_f_folded(L, key, k.x, k.y, fold[e >> vsh], e & m) & m);
+        put(e, prp_f_folded(L, key, k.x, k.y, fold[e >> vsh], e & m) & m);
     }
 }
 
 // n independent blocks per thread per step.  Only the kernels with walk slots
-// in shared memory carry the choice (default 3: config 2 measured 3.01 M
-// trials/s with 2, 3.03 M with 3, 3.02 M with 4); the global-slot kernels keep
-// a plain 2-block fill (cmc_engine below says why).
-template <bool VAR>
+// in shared memory carry the choice (default 3: t = 1024, B = 1536, N = 2^20
+// measured 3.346 M trials/s with 2, 3.354 M with 3, 3.350 M with 4); the
+// global-slot kernels keep a plain 2-block fill (cmc_engine below says why).
+template <bool VAR, bool SHARED>
 __device__ __forceinline__ void fill_round_cache(const Lanes& L, const PrpKey& key,
                                                  const GroupHeader* gh, const uint4* fold,
                                                  uint16_t* cache, uint32_t h, uint32_t m,
                                                  uint32_t gt, uint32_t gthreads, uint32_t n) {
-    if (VAR && n == 4) fill_round_cache_n<4>(L, key, gh, fold, cache, h, m, gt, gthreads);
-    else if (VAR && n != 2) fill_round_cache_n<3>(L, key, gh, fold, cache, h, m, gt, gthreads);
-    else fill_round_cache_n<2>(L, key, gh, fold, cache, h, m, gt, gthreads);
+    if (VAR && n == 4) fill_round_cache_n<4, SHARED>(L, key, gh, fold, cache, h, m, gt, gthreads);
+    else if (VAR && n != 2) fill_round_cache_n<3, SHARED>(L, key, gh, fold, cache, h, m, gt, gthreads);
+    else fill_round_cache_n<2, SHARED>(L, key, gh, fold, cache, h, m, gt, gthreads);
 }
 
 // The fold table of the group's current trial: entry v = (r, y) for Feistel
@@ -531,14 +564,14 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         }
         if (smem_cache) {
             uint16_t* cache = reinterpret_cast<uint16_t*>(gbase + fold_end);
-            fill_round_cache<SMEMSLOTS>(L, key, gh, fold, cache, J.half_bits, (uint32_t)J.mask, gt,
-                                        gthreads, a.fill_blocks);
+            fill_round_cache<SMEMSLOTS, true>(L, key, gh, fold, cache, J.half_bits, (uint32_t)J.mask,
+                                              gt, gthreads, a.fill_blocks);
             group_sync(g, gthreads);
             map_from_cache<MapT>(J, gh, cache, map, lane, a.map_chains ? a.map_chains : 1);
         } else if (glob_cache) {
             uint16_t* gc = a.gcache + (size_t)(blockIdx.x * a.ng + g) * a.gcache_stride;
-            fill_round_cache<SMEMSLOTS>(L, key, gh, fold, gc, J.half_bits, (uint32_t)J.mask, gt,
-                                        gthreads, a.fill_blocks);
+            fill_round_cache<SMEMSLOTS, false>(L, key, gh, fold, gc, J.half_bits, (uint32_t)J.mask,
+                                               gt, gthreads, a.fill_blocks);
             group_sync(g, gthreads);  // orders the group's global writes before its reads
             // four chains hide L2/DRAM latency unless cycle-walking is heavy
             // (c = 2^2h / D > 2), where idle chains' gathers cost more than
@@ -634,8 +667,8 @@ struct Walk {
     static constexpr uint32_t kEmpty = sizeof(BinT) == 2 ? 0xffffu : 0xffffffffu;
 
     SlotMem<MapT, BinT, SMEM> mem;
-    uint64_t walk, rnd, magic, digits;
-    uint32_t magic_shift, k, t, kick, nbins, ndigits;
+    uint64_t walk, rnd, magic, digits, digits_next;
+    uint32_t magic_shift, k, t, kick, nbins, ndigits, ndigits_next;
     uint32_t item, cur, count, phase, choice, target;
     bool bgh, active, failed, bad;
 
@@ -655,8 +688,8 @@ struct Walk {
         magic = k == 3 ? 0xAAAAAAAAAAAAAAABULL : (k == 2 ? 0x8000000000000000ULL : 0x4000000000000000ULL);
         magic_shift = k == 3 ? 1 : 0;
         item = 0; cur = 0; count = 0; phase = 0; choice = 0; target = 0;
-        digits = 0;
-        ndigits = 0;
+        digits = digits_next = 0;
+        ndigits = ndigits_next = 0;
         active = true;
         failed = false;
         bad = false;
@@ -676,7 +709,7 @@ struct Walk {
     // which = r % k; r /= k", cuckoo_core.hpp:126-127), packed 2 bits each.
     // The stream does not depend on the table, so it is decoded ahead of the
     // probes and stays off their load-to-load dependency chain.
-    __device__ __forceinline__ void refill_digits() {
+    __device__ __forceinline__ uint64_t next_digits() {
         uint64_t d = 0;
 #pragma unroll 4
         for (uint32_t i = 0; i < 32; ++i) {
@@ -685,8 +718,18 @@ struct Walk {
             d |= (uint64_t)((uint32_t)rnd - (uint32_t)q * k) << (2 * i);
             rnd = q;
         }
-        digits = d;
-        ndigits = 32;
+        return d;
+    }
+
+    // Keeps at least 32 digits buffered (the current word and the next).
+    // The walker loops call it before every bgh_steps(32): the lanes of a
+    // warp decode their next words together, once per 32 probes, instead of
+    // one lane at a time inside the probe loop with the others waiting.
+    __device__ __forceinline__ void top_up() {
+        if (active && ndigits_next == 0) {
+            digits_next = next_digits();
+            ndigits_next = 32;
+        }
     }
 
     // BGH25 random walk (cuckoo_core.hpp:123-133).  The table write happens
@@ -695,7 +738,11 @@ struct Walk {
     __device__ __forceinline__ void bgh_steps(int n, unsigned long long& probes) {
 #pragma unroll 1
         for (int s = 0; s < n && active; ++s) {
-            if (ndigits == 0) refill_digits();
+            if (ndigits == 0) {
+                digits = digits_next;
+                ndigits = ndigits_next;
+                ndigits_next = 0;
+            }
             const uint32_t which = (uint32_t)digits & 3u;
             digits >>= 2;
             --ndigits;
@@ -805,7 +852,10 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
             w.begin(a, my, a.jobs[job], h);
             busy = true;
         }
-        if (w.bgh) w.bgh_steps(64, probes);
+        if (w.bgh) {
+            w.top_up();
+            w.bgh_steps(32, probes);
+        }
         else w.drrt_steps(64, probes);
         if (busy && !w.active) {
             if (w.bad) {
@@ -892,7 +942,10 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
             w.begin(a, my, a.jobs[job], h);
             busy = true;
         }
-        if (w.bgh) w.bgh_steps(64, probes);
+        if (w.bgh) {
+            w.top_up();
+            w.bgh_steps(32, probes);
+        }
         else w.drrt_steps(64, probes);
         if (busy && !w.active) {
             if (w.bad) {
@@ -995,6 +1048,10 @@ __device__ __forceinline__ void reset_cta_slots(CtaShared* cs) {
 
 template <typename MapT, typename BinT, bool WIDE>
 __global__ void __launch_bounds__(512, 1) cmc_engine_split(const EngineArgs a) {
+    if (!table_base_ok()) {
+        if (threadIdx.x == 0) atomicExch(&a.ctrl->error, kErrBase);
+        return;
+    }
     if (blockIdx.x >= a.producer_ctas) {
         walker_split<MapT, BinT>(a);
         return;
@@ -1018,6 +1075,10 @@ __global__ void __launch_bounds__(512, 1) cmc_engine_split(const EngineArgs a) {
 // fill_blocks choice.
 template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
 __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
+    if (!table_base_ok()) {
+        if (threadIdx.x == 0) atomicExch(&a.ctrl->error, kErrBase);
+        return;
+    }
     char* smem = cmc_dyn_smem;
     build_table(a.t0, smem);
     CtaShared* cs = reinterpret_cast<CtaShared*>(smem + kCtaSharedOff);
@@ -1033,6 +1094,10 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
 // once.
 template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
 __global__ void __launch_bounds__(512, 1) cmc_engine_fused(const __grid_constant__ FusedArgs f) {
+    if (!table_base_ok()) {
+        if (threadIdx.x < f.nclass) atomicExch(&f.cls[threadIdx.x].ctrl->error, kErrBase);
+        return;
+    }
     char* smem = cmc_dyn_smem;
     build_table(f.cls[0].t0, smem);
     CtaShared* cs = reinterpret_cast<CtaShared*>(smem + kCtaSharedOff);
@@ -1137,7 +1202,7 @@ __global__ void cmc_selftest(const uint32_t* t0, const uint32_t* fips_rk, uint32
     const Lanes L{lane * 4, lane * 4 + 128, r256};
     uint32_t c[4];
     encrypt_full(L, fips_rk, 0x00112233u, 0x44556677u, 0x8899aabbu, 0xccddeeffu, c);
-    uint32_t bad = 0;
+    uint32_t bad = table_base_ok() ? 0u : 16u;
     if (c[0] != 0x69c4e0d8u || c[1] != 0x6a7b0430u || c[2] != 0xd8cdb780u || c[3] != 0x70b4c55au)
         bad |= 1;
     // key expansion from words reproduces the FIPS schedule

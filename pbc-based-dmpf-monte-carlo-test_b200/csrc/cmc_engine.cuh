@@ -54,6 +54,15 @@ struct Ctrl {
     unsigned int groups_done;              // split engine: producer groups finished
 };
 
+// What a nonzero Ctrl::error means, for the host's error message.
+inline const char* ctrl_error_text(unsigned int error) {
+    switch (error) {
+    case 3: return "dynamic shared memory does not start where the T-table lookups address it";
+    case 5: return "a device result was out of range";
+    default: return "a bounded device wait gave up";
+    }
+}
+
 // Resident launches: the host publishes work while the kernel runs.  Lives
 // in mapped pinned host memory; the host writes `avail` before `stop`.
 struct ResidentQueue {

@@ -694,8 +694,8 @@ struct Server {
         int rc = cuda(cudaEventSynchronize(b.done), "iteration sync");
         if (rc) return rc;
         if (b.h_ctrl->error)
-            return fail(-int(b.h_ctrl->error), "device wait gave up (site " + std::to_string(b.h_ctrl->where) +
-                                                   "): results discarded");
+            return fail(-int(b.h_ctrl->error), std::string(ctrl_error_text(b.h_ctrl->error)) + " (site " +
+                                                   std::to_string(b.h_ctrl->where) + "): results discarded");
         {
             float t0 = 0, t1 = 0;
             if ((rc = cuda(cudaEventElapsedTime(&t0, origin, b.e0), "engine timing"))) return rc;
@@ -1005,8 +1005,8 @@ struct Server {
         r_stopping = false;
         r_begin = r_avail;  // every published trial was claimed and walked
         if (h_rctrl->error)
-            return fail(-int(h_rctrl->error), "device wait gave up (site " + std::to_string(h_rctrl->where) +
-                                                  "): results discarded");
+            return fail(-int(h_rctrl->error), std::string(ctrl_error_text(h_rctrl->error)) + " (site " +
+                                                  std::to_string(h_rctrl->where) + "): results discarded");
         float t0 = 0, t1 = 0;
         if ((rc = cuda(cudaEventElapsedTime(&t0, origin, r_e0), "engine timing"))) return rc;
         if ((rc = cuda(cudaEventElapsedTime(&t1, origin, r_e1), "engine timing"))) return rc;
