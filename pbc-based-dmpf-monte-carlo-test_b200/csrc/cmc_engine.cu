@@ -721,10 +721,12 @@ struct Walk {
         return d;
     }
 
-    // Keeps at least 32 digits buffered (the current word and the next).
-    // The walker loops call it before every bgh_steps(32): the lanes of a
-    // warp decode their next words together, once per 32 probes, instead of
-    // one lane at a time inside the probe loop with the others waiting.
+    // Keeps at least 32 digits buffered (the current word and the next), for
+    // walks over shared-memory slots.  The walker calls it before every
+    // bgh_steps(32): the lanes of a warp decode their next words together,
+    // once per 32 probes, instead of one lane at a time inside the probe loop
+    // with the others waiting (measured at t = 1024, B = 1536: producers'
+    // waits for a free slot 3.5e9 -> 0.8e9 cycles, 3.36 -> 3.47 M trials/s).
     __device__ __forceinline__ void top_up() {
         if (active && ndigits_next == 0) {
             digits_next = next_digits();
@@ -735,33 +737,48 @@ struct Walk {
     // BGH25 random walk (cuckoo_core.hpp:123-133).  The table write happens
     // on every non-failing probe; on the failing probe the trial ends and its
     // table is never read again, so the write is harmless and unconditional.
+    // Shared-memory slots take their digits from the buffer top_up fills;
+    // global slots keep the digits decoded inside the loop: the walkers over
+    // global slots ran ~3x slower with the buffer (the register-allocation
+    // sensitivity described at cmc_engine below).  Loading the next item's
+    // map entry beside each bin read (it is the next target whenever the bin
+    // is empty) measured 1 % slower on shared slots and is not done.
     __device__ __forceinline__ void bgh_steps(int n, unsigned long long& probes) {
 #pragma unroll 1
         for (int s = 0; s < n && active; ++s) {
             if (ndigits == 0) {
-                digits = digits_next;
-                ndigits = ndigits_next;
-                ndigits_next = 0;
+                if constexpr (SMEM) {
+                    digits = digits_next;
+                    ndigits = ndigits_next;
+                    ndigits_next = 0;
+                } else {
+                    digits = next_digits();
+                    ndigits = 32;
+                }
             }
             const uint32_t which = (uint32_t)digits & 3u;
             digits >>= 2;
             --ndigits;
-            uint32_t tgt = mem.map(cur * k + which);
-            if (tgt >= nbins) {
-                bad = true;
-                tgt = 0;
-            }
-            const uint32_t old = mem.bin(tgt);
-            mem.set(tgt, pack(cur, which));
-            ++probes;
-            const bool empty = old == kEmpty;
-            item += empty;
-            count = empty ? 0 : count + 1;
-            cur = empty ? item : (old & kOrdMask);
-            const bool fail = count > kick || bad;
-            failed = fail;
-            active = !fail && item != t;
+            probe(mem.map(cur * k + which), which, probes);
         }
+    }
+
+    // One probe: copy `which` of item cur goes to bin tgt.
+    __device__ __forceinline__ void probe(uint32_t tgt, uint32_t which, unsigned long long& probes) {
+        if (tgt >= nbins) {
+            bad = true;
+            tgt = 0;
+        }
+        const uint32_t old = mem.bin(tgt);
+        mem.set(tgt, pack(cur, which));
+        ++probes;
+        const bool empty = old == kEmpty;
+        item += empty;
+        count = empty ? 0 : count + 1;
+        cur = empty ? item : (old & kOrdMask);
+        const bool fail = count > kick || bad;
+        failed = fail;
+        active = !fail && item != t;
     }
 
     // DRRT18: one probe per step.
@@ -853,8 +870,12 @@ __device__ __forceinline__ void walker(const EngineArgs& a, CtaShared* cs, uint3
             busy = true;
         }
         if (w.bgh) {
-            w.top_up();
-            w.bgh_steps(32, probes);
+            if constexpr (SMEM) {
+                w.top_up();
+                w.bgh_steps(32, probes);
+            } else {
+                w.bgh_steps(64, probes);
+            }
         }
         else w.drrt_steps(64, probes);
         if (busy && !w.active) {
@@ -942,10 +963,7 @@ __device__ __forceinline__ void walker_split(const EngineArgs& a) {
             w.begin(a, my, a.jobs[job], h);
             busy = true;
         }
-        if (w.bgh) {
-            w.top_up();
-            w.bgh_steps(32, probes);
-        }
+        if (w.bgh) w.bgh_steps(64, probes);
         else w.drrt_steps(64, probes);
         if (busy && !w.active) {
             if (w.bad) {
