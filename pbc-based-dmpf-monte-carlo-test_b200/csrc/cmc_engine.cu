@@ -161,6 +161,12 @@ __device__ __forceinline__ uint32_t div_width(uint32_t y, uint32_t width, uint32
     return q;
 }
 
+// c / k for the copy counts k = 2, 3, 4: 0xAAAAAAAB = ceil(2^33 / 3) with a
+// shift of 33 divides every 32-bit c by 3 exactly; 2 and 4 are shifts.
+__device__ __forceinline__ uint32_t div_k(uint32_t c, uint32_t k) {
+    return k == 3 ? __umulhi(c, 0xAAAAAAABu) >> 1 : c >> (k >> 1);
+}
+
 __device__ __forceinline__ uint32_t find_job(const Job* jobs, uint32_t njobs, uint64_t g) {
     uint32_t lo = 0, hi = njobs;  // last job with trial_base <= g
     while (hi - lo > 1) {
@@ -198,7 +204,7 @@ __device__ __forceinline__ void build_map_direct(const Lanes& L, const Job& J, G
     bool has = c < ncand;
     uint64_t left = 0, right = 0;
     auto start = [&](uint32_t cand) {
-        const uint32_t o = cand / k, j = cand - o * k;
+        const uint32_t o = div_k(cand, k), j = cand - o * k;
         const uint64_t e = sequential ? (uint64_t)o : (shift + (uint64_t)o * step) & range_mask;
         const uint64_t y = e * k + j;
         left = y >> h;
@@ -262,7 +268,7 @@ __device__ __forceinline__ void build_map_cache(const Job& J, GroupHeader* gh,
     uint32_t c[CH], l[CH], r[CH];
     bool has[CH];
     auto start = [&](int i) {
-        const uint32_t o = c[i] / k, j = c[i] - o * k;
+        const uint32_t o = div_k(c[i], k), j = c[i] - o * k;
         const uint64_t e = sequential ? (uint64_t)o : (shift + (uint64_t)o * step) & range_mask;
         const uint32_t y = (uint32_t)(e * k + j);
         l[i] = y >> h;
