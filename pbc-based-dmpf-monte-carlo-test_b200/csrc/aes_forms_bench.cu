@@ -85,8 +85,12 @@ __global__ void __launch_bounds__(384, 1) tt_aes(const __grid_constant__ TtKeys 
         uint32_t s[NB][4];
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            // distinct words in every block: no lookup is shared between blocks
-            s[b][0] = tid; s[b][1] = it * 3u + b; s[b][2] = tid ^ (b << 24); s[b][3] = it ^ (b << 16);
+            // every word is a different sum (carries reach every byte), so the
+            // compiler can prove no two lookups equal: none is shared between
+            // blocks or hoisted out of the loop
+            const uint32_t base = tid * 0x85ebca6bu + it * 0xc2b2ae35u;
+#pragma unroll
+            for (int w = 0; w < 4; ++w) s[b][w] = base + uint32_t(4 * b + w + 1) * 0x9e3779b9u;
         }
 #pragma unroll
         for (int b = 0; b < NB; ++b) tt_block(L, k, s[b]);
