@@ -21,6 +21,8 @@ template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
 __global__ void cmc_engine(const EngineArgs a);
 template <typename MapT, typename BinT, bool WIDE>
 __global__ void cmc_engine_split(const EngineArgs a);
+template <typename MapT, typename BinT>
+__global__ void cmc_engine_pooled(const EngineArgs a);
 template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
 __global__ void cmc_engine_fused(const __grid_constant__ FusedArgs f);
 __global__ void cmc_compact_failures(const uint32_t* bits, uint64_t nbits, uint32_t value_base,
@@ -174,6 +176,16 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     // sub-partitions 0..2 (2 x 7, adding two beside the walker, is within 3%)
     if (pl.isolate && !force_wg) pl.wg = (any_cache || any_gcache) ? 6 : 4;
     if (pl.isolate && pl.nw > 4) pl.nw = 4;
+    // Pooled direct passes (producer_pooled): one-warp groups whose jobs all
+    // use direct passes with 16-bit halves; each group then holds two trials'
+    // headers and staged maps.  Dropped below if the walk slots go global.
+    // Measured on B200 (same failure lists): t=64, B=96 24.4 -> 29.1 M
+    // trials/s; t=27 42.3 -> 58.1 M; t=93 sequential 18.3 -> 20.7 M.
+    pl.pool_stage = 0;
+    if (force_pool != 0 && !any_cache && !any_gcache && !wide_domain && pl.wg == 1 && !pl.walker_ctas) {
+        pl.pool_stage = round_up(max_cand * entry, 16);
+        pl.group_bytes = std::max(pl.group_bytes, pool_group_bytes(pl.pool_stage));
+    }
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
     auto groups_for = [&](uint32_t nw) {
         uint32_t ng = std::min<uint32_t>(kMaxGroups, (16 - nw) / pl.wg);
@@ -235,6 +247,7 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
             pl.ns = ns_g;
         }
     }
+    if (!pl.slots_smem) pl.pool_stage = 0;
     pl.group_off = kEngineTableBytes + kCtaSharedBytes;
     pl.slots_off = pl.group_off + pl.ng * pl.group_bytes;
     pl.smem_bytes = pl.slots_off + (pl.slots_smem ? pl.ns * pl.slot_stride : 0);
@@ -252,11 +265,12 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     char buf[256];
     snprintf(buf, sizeof buf,
              "engine=%s variant=%s groups=%u warps_per_group=%u walkers=%u%s slots=%u slots_in=%s "
-             "smem=%u threads=%u ctas=%u cache=%s",
+             "smem=%u threads=%u ctas=%u cache=%s%s",
              pl.walker_ctas ? "split" : "group", pl.variant == 0 ? "narrow" : pl.variant == 1 ? "wide" : "wide-domain", pl.ng, pl.wg,
              pl.walker_ctas ? pl.walker_ctas : pl.nw, pl.isolate ? "(isolated)" : "", pl.ns,
              pl.slots_smem ? "smem" : "global", pl.smem_bytes, pl.threads, pl.ctas,
-             any_cache && any_gcache ? "smem+global" : any_cache ? "smem" : any_gcache ? "global" : "off");
+             any_cache && any_gcache ? "smem+global" : any_cache ? "smem" : any_gcache ? "global" : "off",
+             pl.pool_stage ? " pooled" : "");
     plan_text = buf;
     return CMC_OK;
 }
@@ -362,17 +376,19 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
         a.idle_polls = spin_limit;
         a.map_chains = map_chains;
         a.fill_blocks = fill_blocks;
+        a.pool_stage = pl.pool_stage;
         return a;
     };
     // Fused: one launch per entry width that two or more classes share (the
     // width is a template parameter of the engine), in the order of each
     // width's heaviest class; a class alone in its width runs by itself.
     std::vector<bool> launched(nclass, false);
+    // Classes with pooled direct passes run their own kernel, unfused.
     for (uint32_t lead = 0; lead < nclass && fuse; ++lead) {
-        if (launched[lead]) continue;
+        if (launched[lead] || plans[lead].pool_stage) continue;
         std::vector<uint32_t> members;
         for (uint32_t c = lead; c < nclass; ++c)
-            if (!launched[c] && plans[c].variant == plans[lead].variant &&
+            if (!launched[c] && !plans[c].pool_stage && plans[c].variant == plans[lead].variant &&
                 plans[c].slots_smem == plans[lead].slots_smem)
                 members.push_back(c);
         if (members.size() < 2) continue;
@@ -411,7 +427,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
                 ? (pl.variant == 0   ? (const void*)cmc_engine_split<uint16_t, uint16_t, false>
                    : pl.variant == 1 ? (const void*)cmc_engine_split<uint32_t, uint32_t, false>
                                      : (const void*)cmc_engine_split<uint32_t, uint32_t, true>)
-                : engine_kernel(pl.variant, pl.slots_smem);
+                : engine_kernel(pl.variant, pl.slots_smem, pl.pool_stage != 0);
         void* args[] = {&a};
         // The split engine's producer and walker CTAs hand trials to each other, so
         // they must all be resident at once: a cooperative launch guarantees it.
@@ -460,7 +476,10 @@ int Ctx::check_ctrl() {
     return CMC_OK;
 }
 
-const void* engine_kernel(int variant, bool smem_slots) {
+const void* engine_kernel(int variant, bool smem_slots, bool pooled) {
+    if (pooled && smem_slots && variant != 2)
+        return variant == 0 ? (const void*)cmc_engine_pooled<uint16_t, uint16_t>
+                            : (const void*)cmc_engine_pooled<uint32_t, uint32_t>;
     if (smem_slots)
         return variant == 0   ? (const void*)cmc_engine<uint16_t, uint16_t, false, true>
                : variant == 1 ? (const void*)cmc_engine<uint32_t, uint32_t, false, true>
@@ -491,7 +510,8 @@ int engine_smem_cap(size_t optin) {
                          (const void*)cmc_engine_split<uint32_t, uint32_t, true>,
                          fused_engine_kernel(0, true), fused_engine_kernel(1, true),
                          fused_engine_kernel(2, true), fused_engine_kernel(0, false),
-                         fused_engine_kernel(1, false), fused_engine_kernel(2, false)};
+                         fused_engine_kernel(1, false), fused_engine_kernel(2, false),
+                         engine_kernel(0, true, true), engine_kernel(1, true, true)};
     for (const void* fn : fns)
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(optin)) != cudaSuccess)
             return CMC_ECUDA;
@@ -1028,6 +1048,7 @@ int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value) {
     else if (n == "groups" && value >= 0 && value <= cmc::kMaxGroups) c->force_ng = uint32_t(value);
     else if (n == "global_slots" && (value == 0 || value == 1)) c->force_global_slots = uint32_t(value);
     else if (n == "method" && value >= -1 && value <= 2) c->force_method = int(value);
+    else if (n == "pool" && value >= -1 && value <= 1) c->force_pool = int(value);
     else if (n == "graph" && (value == 0 || value == 1)) c->use_graphs = int(value);
     else if (n == "fused" && (value == 0 || value == 1)) c->use_fused = int(value);
     else if (n == "fill_blocks" && (value == 0 || (value >= 2 && value <= 4))) c->fill_blocks = uint32_t(value);

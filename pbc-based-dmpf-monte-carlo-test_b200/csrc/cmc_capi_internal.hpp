@@ -26,6 +26,7 @@ struct Plan {
     uint64_t gslot_bytes = 0;     // global walk slots (0: slots in shared memory)
     uint32_t gcache_stride = 0;   // u16 entries per group's global round cache
     uint64_t gcache_bytes = 0;    // all groups' global round caches
+    uint32_t pool_stage = 0;      // pooled direct passes: bytes per staging map (0: off)
 };
 
 uint32_t choose_method(uint32_t h, uint64_t domain, double candidates, int force, bool may_allocate);
@@ -33,7 +34,7 @@ uint32_t choose_method(uint32_t h, uint64_t domain, double candidates, int force
 int engine_smem_cap(size_t optin);
 // The engine kernel for a plan's entry width (Plan::variant) and walk-slot
 // placement, and the fused kernel of the same kind.
-const void* engine_kernel(int variant, bool smem_slots);
+const void* engine_kernel(int variant, bool smem_slots, bool pooled = false);
 const void* fused_engine_kernel(int variant, bool smem_slots);
 // Estimated cost of one trial in AES-block equivalents (seeds, map, 0.1 t for the walk).
 double job_cost(const Job& j);
@@ -97,6 +98,7 @@ struct Ctx {
     uint32_t* h_nf = nullptr;                // pinned failure count of the last batched call
     std::string graph_state;                 // "eager", "captured" or "replayed"
     int force_method = -1;  // -1 auto, 0 direct, 1 cache (shared if h <= 12, else global), 2 global cache
+    int force_pool = -1;    // pooled direct passes: -1 auto, 0 off, 1 on where they apply
     bool may_allocate = true;  // false: no global round cache, global slots only if unavoidable
     uint32_t spin_limit = 1u << 26;
     uint32_t map_chains = 0;  // lookup chains per lane from a round cache (0: automatic)

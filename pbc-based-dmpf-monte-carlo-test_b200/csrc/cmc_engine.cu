@@ -45,6 +45,7 @@ struct GroupHeader {
     uint32_t r1[8][8];  // Round1 {c0, w3hi, c1, c2, c3} per Feistel round (padded)
     unsigned long long walk, rnd, shift, step;
     uint32_t slot, cand_next, abort, live;
+    uint32_t done;             // pooled direct passes: candidates whose bucket is staged
     unsigned long long entry;  // resident launch: ring entry of the last trial
     unsigned long long avail;  // resident launch: the last published end this group read
     Job jd;                    // this trial's job descriptor, read at L2
@@ -622,6 +623,213 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
     }
 }
 
+// Pooled direct passes for one-warp groups (the planner sets pool_stage only
+// for launches whose jobs all use direct passes with 16-bit Feistel halves,
+// walk slots in shared memory and no resident queue).  With one trial at a
+// time, the last Feistel passes of each trial run with most lanes idle: the
+// number of passes per candidate is geometric (cycle-walking), so a warp of
+// 32 lanes on 192 candidates keeps ~78 % of its lanes busy.  Here the warp
+// holds kPoolContexts trials: a lane whose context has no candidate left
+// takes one from the other, loading that trial's key when it switches, and a
+// finished trial is published (its staged map copied into a free slot) and
+// replaced by the next one at the top of the loop, where the warp is
+// converged.  A slot is held only while its map is copied.
+template <typename MapT, typename BinT>
+__device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem, CtaShared* cs, uint32_t g,
+                                                uint32_t lane) {
+    const Lanes L{lane * 4, lane * 4 + 128, a.r256};
+    char* gbase = smem + a.group_off + g * a.group_bytes;
+    auto ctx = [&](uint32_t j) { return reinterpret_cast<GroupHeader*>(gbase + j * kPoolHeaderStride); };
+    auto stage = [&](uint32_t j) {
+        return reinterpret_cast<MapT*>(gbase + kPoolContexts * kPoolHeaderStride + j * a.pool_stage);
+    };
+    const unsigned long long total = a.total_dev ? *a.total_dev : a.total;
+    if (lane < kPoolContexts) ctx(lane)->live = 0;
+    __syncwarp();
+    bool more = true, abort = false;
+    uint32_t cursor = g;
+    // this lane's trial parameters (those of context kj) and candidate
+    int kj = -1, cj = -1;
+    PrpKey key;
+    uint32_t h = 0, mask = 0, kk = 0, width = 0, wmagic = 0, c = 0, l = 0, r = 0;
+    uint64_t domain = 0, shift = 0, step = 0, rmask = 0;
+    bool sequential = false;
+    for (;;) {
+        // converged: publish finished trials, start new ones
+#pragma unroll 1
+        for (uint32_t j = 0; j < kPoolContexts && !abort; ++j) {
+            GroupHeader* gh = ctx(j);
+            if (gh->live && gh->done == gh->jd.pnum * gh->jd.k) {
+                const uint32_t ncand = gh->jd.pnum * gh->jd.k;
+                uint32_t slot = 0;
+                if (lane == 0) {
+                    const long long wait0 = clock64();
+                    const unsigned long long wait_ns = globaltimer_ns();
+                    slot = 0xffffffffu;
+                    for (;;) {
+                        for (uint32_t i = 0; i < a.ns; ++i) {
+                            const uint32_t sidx = (cursor + i) % a.ns;
+                            if (atomicCAS(&cs->slot_state[sidx], kSlotFree, kSlotFilling) == kSlotFree) {
+                                slot = sidx;
+                                break;
+                            }
+                        }
+                        if (slot != 0xffffffffu) break;
+                        __nanosleep(128);
+                        if (globaltimer_ns() - wait_ns > 1000ULL * a.spin_limit) {
+                            atomicExch(&a.ctrl->error, kErrTimeout);
+                            atomicExch(&a.ctrl->where, 1u);
+                            break;
+                        }
+                    }
+                    atomicAdd(&a.ctrl->slot_wait_cycles, (unsigned long long)(clock64() - wait0));
+                }
+                slot = __shfl_sync(kFull, slot, 0);
+                if (slot == 0xffffffffu) {
+                    abort = true;
+                    break;
+                }
+                cursor = slot + 1;
+                char* sbase = smem + a.slots_off + (size_t)slot * a.slot_stride;
+                {
+                    const uint32_t nvec = (gh->jd.buckets * (uint32_t)sizeof(BinT) + 15) / 16;
+                    uint4* b4 = reinterpret_cast<uint4*>(sbase);
+                    for (uint32_t i = lane; i < nvec; i += 32) b4[i] = make_uint4(kFull, kFull, kFull, kFull);
+                    MapT* map = reinterpret_cast<MapT*>(sbase + a.bins_bytes);
+                    const MapT* st = stage(j);
+                    for (uint32_t i = lane; i < ncand; i += 32) map[i] = st[i];
+                }
+                __syncwarp();
+                __threadfence_block();
+                if (lane == 0) {
+                    SlotHeader& sh = cs->slot_hdr[slot];
+                    sh.gidx = gh->gidx;
+                    sh.walk = gh->walk;
+                    sh.rnd = gh->rnd;
+                    sh.job = gh->job;
+                    sh.offset = gh->offset;
+                    st_release(&cs->slot_state[slot], kSlotReady);
+                    gh->live = 0;
+                }
+                if (kj == (int)j) kj = -1;  // the context's next trial has another key
+                __syncwarp();
+            }
+            if (!gh->live && more) {
+                if (lane == 0) {
+                    const unsigned long long gi = a.gidx_begin + atomicAdd(&a.ctrl->next, 1ULL);
+                    gh->gidx = gi;
+                    gh->abort = gi < total;  // here: the claim holds a trial
+                    if (gi < total) {
+                        const uint32_t jb = find_job(a.jobs, a.njobs, gi);
+                        gh->job = jb;
+                        gh->offset = a.jobs[jb].first + (uint32_t)(gi - a.jobs[jb].trial_base);
+                    }
+                }
+                __syncwarp();
+                if (!gh->abort) {
+                    more = false;
+                    continue;
+                }
+                {
+                    const uint32_t* src = reinterpret_cast<const uint32_t*>(&a.jobs[gh->job]);
+                    uint32_t* dst = reinterpret_cast<uint32_t*>(&gh->jd);
+                    for (uint32_t i = lane; i < sizeof(Job) / 4; i += 32) dst[i] = __ldcg(src + i);
+                }
+                __syncwarp();
+                const Job& J = gh->jd;
+                // per-trial PRP key (lane 0) and walk seed (lane 1), cuckoo_bench.cu:226-238
+                if (lane == 0) {
+                    uint32_t w[4];
+                    encrypt_full(L, J.batch_rk, 0x4b455931u, 0, gh->offset, 0x50525031u, w);
+                    expand_key(L, w[0], w[1], w[2], w[3], gh->rk);
+                } else if (lane == 1) {
+                    uint32_t w[4];
+                    encrypt_full(L, J.batch_rk, 0x57414c4bu, 0, gh->offset, 0x524e4731u, w);
+                    uint64_t walk = ((uint64_t)w[0] << 32) | w[1];
+                    const uint64_t sh = (((uint64_t)w[2] << 32) | w[3]) & J.range_mask;
+                    uint64_t input_state = sh ^ 0xd1b54a32d192ed03ULL;
+                    gh->step = (splitmix(input_state) | 1ULL) & J.range_mask;
+                    gh->shift = sh;
+                    gh->rnd = splitmix(walk);
+                    gh->walk = walk;
+                    gh->cand_next = 0;
+                    gh->done = 0;
+                }
+                __syncwarp();
+                if (lane < 8) {
+                    const Round1 rc = round1_consts(L, gh->rk, lane, J.half_bits);
+                    gh->r1[lane][0] = rc.c0; gh->r1[lane][1] = rc.w3hi; gh->r1[lane][2] = rc.c1;
+                    gh->r1[lane][3] = rc.c2; gh->r1[lane][4] = rc.c3;
+                }
+                __syncwarp();
+                if (lane == 0) gh->live = 1;
+                __syncwarp();
+            }
+        }
+        if (abort) break;
+        bool any_live = false;
+        for (uint32_t j = 0; j < kPoolContexts; ++j) any_live |= ctx(j)->live != 0;
+        if (!any_live) break;
+        // lanes without a candidate take one, from the contexts in order
+#pragma unroll 1
+        for (uint32_t j = 0; j < kPoolContexts; ++j) {
+            GroupHeader* gh = ctx(j);
+            const bool need = cj < 0 && gh->live;
+            const uint32_t nc = claim(&gh->cand_next, need, lane);
+            if (need && nc < gh->jd.pnum * gh->jd.k) {
+                cj = (int)j;
+                c = nc;
+                if (kj != (int)j) {
+                    const Job& J = gh->jd;
+                    prp_key_from_schedule(gh->rk, key);
+                    h = J.half_bits;
+                    mask = (uint32_t)J.mask;
+                    domain = J.domain;
+                    kk = J.k;
+                    width = (uint32_t)J.width;
+                    wmagic = J.width_magic;
+                    sequential = J.input_mode == 0;
+                    shift = gh->shift;
+                    step = gh->step;
+                    rmask = J.range_mask;
+                    kj = (int)j;
+                }
+                const uint32_t o = div_k(c, kk), jc = c - o * kk;
+                const uint64_t e = sequential ? (uint64_t)o : (shift + (uint64_t)o * step) & rmask;
+                const uint32_t y = (uint32_t)(e * kk + jc);
+                l = y >> h;
+                r = y & mask;
+            }
+        }
+        // one Feistel pass (8 rounds) per lane with a candidate
+        if (cj >= 0) {
+            const GroupHeader* gh = ctx((uint32_t)cj);
+#pragma unroll 1
+            for (uint32_t rr = 0; rr < 8; ++rr) {
+                const Round1 rc = load_round1(gh, rr);
+                const uint32_t f = prp_f(L, key, rc, r) & mask;
+                const uint32_t nr = (l ^ f) & mask;
+                l = r;
+                r = nr;
+            }
+            const uint32_t y = (l << h) | r;
+            if (y < domain) {
+                stage((uint32_t)cj)[c] = (MapT)div_width(y, width, wmagic);
+                atomicAdd(&ctx((uint32_t)cj)->done, 1u);
+                cj = -1;
+            } else {
+                l = y >> h;
+                r = y & mask;
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        __threadfence_block();
+        atomicAdd(&cs->groups_done, 1u);
+    }
+}
+
 // ------------------------------------------------------------------ walker --
 
 // Slot storage seen by one walker lane: shared-memory offsets (loads compile
@@ -1042,7 +1250,7 @@ __device__ __forceinline__ void build_table(const uint32_t* t0, char* smem) {
 // share their issue slots with few or no throughput-bound AES warps.  Warps
 // with no role return at once.  SMEMSLOTS: the plan keeps its walk slots in
 // shared memory (a.gslots null) or, if false, in global memory.
-template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS>
+template <typename MapT, typename BinT, bool WIDE, bool SMEMSLOTS, bool POOL = false>
 __device__ __forceinline__ void engine_roles(const EngineArgs& a, char* smem, CtaShared* cs) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t producer_idx = 0xffffffffu, walker_idx = 0xffffffffu;
@@ -1057,7 +1265,8 @@ __device__ __forceinline__ void engine_roles(const EngineArgs& a, char* smem, Ct
     }
     if (producer_idx < a.ng * a.wg) {
         const uint32_t g = producer_idx / a.wg;
-        producer<MapT, BinT, WIDE, false, SMEMSLOTS>(a, smem, cs, g, (producer_idx % a.wg) * 32 + lane);
+        if constexpr (POOL) producer_pooled<MapT, BinT>(a, smem, cs, g, lane);
+        else producer<MapT, BinT, WIDE, false, SMEMSLOTS>(a, smem, cs, g, (producer_idx % a.wg) * 32 + lane);
     } else if (walker_idx < a.nw) {
         walker<MapT, BinT, SMEMSLOTS>(a, cs, walker_idx);
     }
@@ -1109,6 +1318,23 @@ __global__ void __launch_bounds__(512, 1) cmc_engine(const EngineArgs a) {
     reset_cta_slots(cs);
     __syncthreads();
     engine_roles<MapT, BinT, WIDE, SMEMSLOTS>(a, smem, cs);
+}
+
+// Pooled direct passes (producer_pooled): 16-bit Feistel halves, walk slots in
+// shared memory.  A kernel of its own, so that the other kernels' register
+// allocation is unchanged.
+template <typename MapT, typename BinT>
+__global__ void __launch_bounds__(512, 1) cmc_engine_pooled(const EngineArgs a) {
+    if (!table_base_ok()) {
+        if (threadIdx.x == 0) atomicExch(&a.ctrl->error, kErrBase);
+        return;
+    }
+    char* smem = cmc_dyn_smem;
+    build_table(a.t0, smem);
+    CtaShared* cs = reinterpret_cast<CtaShared*>(smem + kCtaSharedOff);
+    reset_cta_slots(cs);
+    __syncthreads();
+    engine_roles<MapT, BinT, false, true, true>(a, smem, cs);
 }
 
 // Plan classes of a batched call in one launch (FusedArgs in cmc_engine.cuh),
@@ -1263,6 +1489,8 @@ template __global__ void cmc_engine<uint32_t, uint32_t, true, true>(const Engine
 template __global__ void cmc_engine<uint16_t, uint16_t, false, false>(const EngineArgs);
 template __global__ void cmc_engine<uint32_t, uint32_t, false, false>(const EngineArgs);
 template __global__ void cmc_engine<uint32_t, uint32_t, true, false>(const EngineArgs);
+template __global__ void cmc_engine_pooled<uint16_t, uint16_t>(const EngineArgs);
+template __global__ void cmc_engine_pooled<uint32_t, uint32_t>(const EngineArgs);
 template __global__ void cmc_engine_split<uint16_t, uint16_t, false>(const EngineArgs);
 template __global__ void cmc_engine_split<uint32_t, uint32_t, false>(const EngineArgs);
 template __global__ void cmc_engine_split<uint32_t, uint32_t, true>(const EngineArgs);

@@ -19,6 +19,16 @@ constexpr uint32_t kEngineTableBytes = 65536;  // replicated T-table at shared o
 constexpr uint32_t kMaxGroups = 14; // named barriers 1..14
 constexpr uint32_t kGroupHeaderBytes = 1024;  // per-group shared header (the trial's job copy)
 
+// Pooled direct passes (EngineArgs::pool_stage != 0): a one-warp group keeps
+// kPoolContexts trials in flight, each with its own header (kPoolHeaderStride
+// apart: 16 bytes more than a header, so the contexts' round constants fall in
+// different banks) and a staging map of pool_stage bytes after the headers.
+constexpr uint32_t kPoolContexts = 2;
+constexpr uint32_t kPoolHeaderStride = kGroupHeaderBytes + 16;
+__host__ __device__ constexpr uint32_t pool_group_bytes(uint32_t stage) {
+    return kPoolContexts * (kPoolHeaderStride + stage);
+}
+
 // A group's shared region: [header, kGroupHeaderBytes][round-2 fold table of a
 // round-cache job][the round cache itself, when it is kept in shared memory].
 // The fold table holds 8 rounds x 2^max(0, h - 8) entries of 16 bytes.
@@ -122,6 +132,7 @@ struct EngineArgs {
     uint32_t ring_mask;
     uint32_t map_chains;                // lookup chains per lane from a round cache (0: automatic)
     uint32_t fill_blocks;               // round-cache fill: blocks per thread per step (0: automatic)
+    uint32_t pool_stage;                // pooled direct passes: bytes per staging map (0: off)
     unsigned long long entry_begin;
     unsigned long long bits_mask;
     unsigned int* entry_done;

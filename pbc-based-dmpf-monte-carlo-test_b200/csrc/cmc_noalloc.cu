@@ -204,7 +204,9 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
     a.slots_off = pl.slots_off;
     a.spin_limit = pl_ctx.spin_limit;
     a.idle_polls = pl_ctx.spin_limit;
-    const void* fn = engine_kernel(pl.variant, true);  // walk slots in shared memory (checked above)
+    a.pool_stage = pl.pool_stage;
+    // walk slots in shared memory (checked above)
+    const void* fn = engine_kernel(pl.variant, true, pl.pool_stage != 0);
     // the engine's shared-memory limit was raised to the device maximum at set-up
     void* args[] = {&a};
     e = cudaLaunchKernel(fn, dim3(pl.ctas), dim3(pl.threads), args, pl.smem_bytes, s);

@@ -657,7 +657,8 @@ struct Server {
         a.idle_polls = ctx->spin_limit;
         a.map_chains = ctx->map_chains;
         a.fill_blocks = ctx->fill_blocks;
-        const void* fn = engine_kernel(pl.variant, pl.slots_smem);
+        a.pool_stage = pl.pool_stage;
+        const void* fn = engine_kernel(pl.variant, pl.slots_smem, pl.pool_stage != 0);
         // the context raised the engine's shared-memory limit to the device maximum
         void* args[] = {&a};
         if ((rc = cuda(cudaEventRecord(b.e0, st), "event"))) return rc;
@@ -980,6 +981,7 @@ struct Server {
         a.spin_limit = ctx->spin_limit;
         a.map_chains = ctx->map_chains;
         a.fill_blocks = ctx->fill_blocks;
+        // the resident launch claims trials from the host's ring: plain producers
         const void* fn = engine_kernel(pl.variant, pl.slots_smem);
         // the context raised the engine's shared-memory limit to the device maximum
         void* args[] = {&a};

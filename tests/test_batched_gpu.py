@@ -66,10 +66,12 @@ def test_plan_classes(ctx, cmc, fused):
     # (fused, the default) or one launch per class
     jobs = plan_class_jobs(cmc)
     ctx.set_option("fused", fused)
+    ctx.set_option("pool", 0)   # the t = 64 class would take pooled passes, unfused
     try:
         failed, per_job = ctx.run_jobs(jobs)
     finally:
         ctx.set_option("fused", 1)
+        ctx.set_option("pool", -1)
     assert " | " in ctx.last_plan
     if fused:
         # classes of one entry width and walk-slot placement share a launch:
@@ -89,7 +91,11 @@ def test_fused_with_other_entry_width(ctx, cmc):
     # and runs by itself too; every job as alone
     jobs = plan_class_jobs(cmc)[1:] + [
         (cmc.parameters("bgh25", 50000, 20, 3, 70000, 50, "affine"), 9, 0, 0, 8)]
-    failed, per_job = ctx.run_jobs(jobs)
+    ctx.set_option("pool", 0)
+    try:
+        failed, per_job = ctx.run_jobs(jobs)
+    finally:
+        ctx.set_option("pool", -1)
     assert ctx.last_plan.startswith("fused(") and ctx.last_kernel_count == 4
     for i, (p, s, b, first, count) in enumerate(jobs):
         assert per_job[i] == ctx.launch(p, cmc.batch_key(s, b), first, count), i
@@ -132,3 +138,17 @@ def test_graph_capture_and_replay(ctx, cmc):
         assert "graph=" not in ctx.last_plan
     finally:
         ctx.set_option("graph", 1)
+
+
+def test_pooled_class_runs_unfused(ctx, cmc):
+    # the t = 64 class takes pooled direct passes in a kernel of its own; the
+    # two global-slot classes share a fused launch and the t = 300 class, alone
+    # in its kind, runs by itself: four kernels with the compaction, and every
+    # job as alone
+    jobs = plan_class_jobs(cmc)
+    failed, per_job = ctx.run_jobs(jobs)
+    assert "pooled" in ctx.last_plan
+    assert ctx.last_kernel_count == 4
+    for i, (p, s, b, first, count) in enumerate(jobs):
+        assert per_job[i] == ctx.launch(p, cmc.batch_key(s, b), first, count), i
+

@@ -24,11 +24,12 @@ ENGINE_VARIANTS = [
     {"method": 1, "map_chains": 2},            # two lookup chains per lane (shared cache)
     {"method": 2, "map_chains": 1},
     {"method": 2, "map_chains": 4},
+    {"pool": 1, "warps_per_group": 1, "method": 0},   # pooled direct passes (two trials per warp)
 ]
 
 
 DEFAULTS = {"method": -1, "global_slots": 0, "warps_per_group": 0, "groups": 0, "walkers": 0,
-            "walker_ctas": -1, "isolate_walkers": -1, "map_chains": 0}
+            "walker_ctas": -1, "isolate_walkers": -1, "map_chains": 0, "pool": -1}
 
 
 def apply(ctx, opts):
@@ -115,7 +116,7 @@ def random_shapes(n, seed):
 @pytest.mark.parametrize("shape", random_shapes(24, 7))
 def test_vs_oracle_random_shapes(ctx, cmc, oracle, shape):
     mode, im, pnum, ell, k, buckets, kick, seed, batch = shape
-    apply(ctx, ENGINE_VARIANTS[[0, 6, 7, 9, 10, 11, 12, 13, 15][seed % 9]])
+    apply(ctx, ENGINE_VARIANTS[[0, 6, 7, 9, 10, 11, 12, 13, 15, 16][seed % 10]])
     p = cmc.parameters(mode, pnum, ell, k, buckets, kick, im)
     op = oracle.params(mode, pnum, ell, k, buckets, kick, im)
     count = 512 if pnum <= 100 else 96
@@ -190,3 +191,26 @@ def test_full_batch_properties(ctx, cmc):
         parts += ctx.launch(p, key, off, min(3 << 14, n - off))
     assert parts == whole
     assert len(whole) > 0
+
+
+@pytest.mark.parametrize("shape", [
+    # mode, input, t, ell_i, k, B, kick  (direct passes, shared walk slots)
+    ("bgh25", "affine", 64, 16, 3, 96, 100),       # config-1 table
+    ("bgh25", "affine", 64, 16, 3, 70, 20),        # failing often
+    ("drrt18", "affine", 64, 16, 3, 80, 20),
+    ("bgh25", "sequential", 27, 12, 2, 30, 5),
+    ("bgh25", "affine", 300, 20, 4, 330, 50),
+    ("drrt18", "sequential", 5, 8, 3, 6, 5),       # fewer candidates than lanes
+])
+def test_pooled_direct_passes_vs_oracle(ctx, cmc, oracle, shape):
+    # two trials in flight per one-warp group, maps staged and copied into
+    # slots at publish time: every trial's outcome as the oracle has it
+    mode, im, pnum, ell, k, buckets, kick = shape
+    apply(ctx, {"pool": 1, "warps_per_group": 1, "method": 0})
+    p = cmc.parameters(mode, pnum, ell, k, buckets, kick, im)
+    op = oracle.params(mode, pnum, ell, k, buckets, kick, im)
+    want = oracle.batch(op, 11, 2, 5, 3000)
+    got = ctx.launch(p, cmc.batch_key(11, 2), 5, 3000)
+    assert "pooled" in ctx.last_plan, ctx.last_plan
+    assert got == want, (shape, ctx.last_plan)
+
