@@ -211,7 +211,12 @@ int cmc_server_destroy(cmc_server* server);
  * move to the class with the most work left; 0: one launch per class),
  * "fill_blocks" (0 automatic, or 2..4: AES blocks each thread keeps in flight
  * while filling a round cache, in plans whose walk slots are in shared
- * memory; automatic is 3 there and 2 elsewhere).
+ * memory; automatic is 3 there and 2 elsewhere), "pool" (-1, the default:
+ * one-warp groups whose jobs all take direct passes with 16-bit Feistel
+ * halves and shared-memory walk slots keep two trials in flight and stage
+ * their maps; 0: one trial at a time; 1 as -1 -- such plans run in a kernel
+ * of their own, outside fused launches, and resident server launches never
+ * pool).
  * Returns CMC_EINVAL for an unknown name or a value out of range. */
 int cmc_set_option(cmc_ctx* ctx, const char* name, int64_t value);
 
