@@ -213,7 +213,7 @@ int cmc_server_destroy(cmc_server* server);
  * while filling a round cache, in plans whose walk slots are in shared
  * memory; automatic is 3 there and 2 elsewhere), "pool" (-1, the default:
  * one-warp groups whose jobs all take direct passes with 16-bit Feistel
- * halves and shared-memory walk slots keep two trials in flight and stage
+ * halves and shared-memory walk slots keep three trials in flight and stage
  * their maps; 0: one trial at a time; 1 as -1 -- such plans run in a kernel
  * of their own, outside fused launches, and resident server launches never
  * pool).

@@ -160,7 +160,10 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     const uint32_t gfold_bytes = any_gcache ? fold_table_bytes(max_gcache_h) : 0;
     pl.group_bytes = kGroupHeaderBytes + std::max(cache_bytes, gfold_bytes);
     const double avg_cand = work > 0 ? cand_work / work : 0;
-    pl.wg = (any_cache || any_gcache || avg_cand >= 768.0) ? 4 : 1;
+    // one-warp groups for direct passes up to 1,536 candidates per trial (with
+    // pooled passes, measured: t=300 k=3 6.75 M trials/s against 5.14 M in
+    // 4-warp groups; t=1000: 1.57 M against 1.61 M)
+    pl.wg = (any_cache || any_gcache || avg_cand >= 1536.0) ? 4 : 1;
     if (force_wg) pl.wg = force_wg;
     pl.walker_ctas = force_walker_ctas > 0 ? uint32_t(force_walker_ctas) : 0;
     if (pl.walker_ctas >= uint32_t(sms)) return fail(CMC_EINVAL, "walker_ctas must be below the SM count");
@@ -177,7 +180,7 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     if (pl.isolate && !force_wg) pl.wg = (any_cache || any_gcache) ? 6 : 4;
     if (pl.isolate && pl.nw > 4) pl.nw = 4;
     // Pooled direct passes (producer_pooled): one-warp groups whose jobs all
-    // use direct passes with 16-bit halves; each group then holds two trials'
+    // use direct passes with 16-bit halves; each group then holds three trials'
     // headers and staged maps.  Dropped below if the walk slots go global.
     // Measured on B200 (same failure lists): t=64, B=96 24.4 -> 29.1 M
     // trials/s; t=27 42.3 -> 58.1 M; t=93 sequential 18.3 -> 20.7 M.

@@ -630,7 +630,7 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
 // number of passes per candidate is geometric (cycle-walking), so a warp of
 // 32 lanes on 192 candidates keeps ~78 % of its lanes busy.  Here the warp
 // holds kPoolContexts trials: a lane whose context has no candidate left
-// takes one from the other, loading that trial's key when it switches, and a
+// takes one from the next, loading that trial's key when it switches, and a
 // finished trial is published (its staged map copied into a free slot) and
 // replaced by the next one at the top of the loop, where the warp is
 // converged.  A slot is held only while its map is copied.

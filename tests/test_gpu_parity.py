@@ -24,7 +24,7 @@ ENGINE_VARIANTS = [
     {"method": 1, "map_chains": 2},            # two lookup chains per lane (shared cache)
     {"method": 2, "map_chains": 1},
     {"method": 2, "map_chains": 4},
-    {"pool": 1, "warps_per_group": 1, "method": 0},   # pooled direct passes (two trials per warp)
+    {"pool": 1, "warps_per_group": 1, "method": 0},   # pooled direct passes (three trials per warp)
 ]
 
 
@@ -203,7 +203,7 @@ def test_full_batch_properties(ctx, cmc):
     ("drrt18", "sequential", 5, 8, 3, 6, 5),       # fewer candidates than lanes
 ])
 def test_pooled_direct_passes_vs_oracle(ctx, cmc, oracle, shape):
-    # two trials in flight per one-warp group, maps staged and copied into
+    # three trials in flight per one-warp group, maps staged and copied into
     # slots at publish time: every trial's outcome as the oracle has it
     mode, im, pnum, ell, k, buckets, kick = shape
     apply(ctx, {"pool": 1, "warps_per_group": 1, "method": 0})
