@@ -388,7 +388,7 @@ def run_reference_gpu_arm(args, rank: int, world: int) -> None:
 # ------------------------------------------------- other single-set workloads --
 
 def workload_summary(cmc, ctx, w: dict, sms: int, max_mhz: float, steps: int = 4,
-                     warmup: int = 3) -> dict:
+                     warmup: int = 3, name: str | None = None) -> dict:
     """A compact line for another single-configuration workload, measured after
     the main timed region: device-resident launches over batches warmup..,
     timed with CUDA events (L2 flushed between steps), the roofline fraction,
@@ -437,7 +437,7 @@ def workload_summary(cmc, ctx, w: dict, sms: int, max_mhz: float, steps: int = 4
             "e2e": {"value": e2e, "unit": "trials/s",
                     "timing": "host wall clock around one cmc_launch with host buffers"},
             "roofline": {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak},
+                         "frac": achieved / peak, "traffic": read_traffic(name) if name else None},
             "plan": ctx.last_plan, "cpu_baseline": base,
             "parity": parity_check(ctx, cmc, w, n_cpu, cpu_fails, base["kind"])}
 
@@ -828,8 +828,10 @@ def main():
         if world == 1 and args.workload == "config2" and not args.no_extras:
             # the batching and serving patterns, measured on the same box after
             # the timed region (own contexts; bounded to about a minute each)
-            for name, fn in (("config1", lambda c: workload_summary(cmc, c, WORKLOADS["config1"], sms, max_mhz)),
-                             ("config4", lambda c: workload_summary(cmc, c, WORKLOADS["config4"], sms, max_mhz)),
+            for name, fn in (("config1", lambda c: workload_summary(cmc, c, WORKLOADS["config1"], sms, max_mhz,
+                                                                    name="config1")),
+                             ("config4", lambda c: workload_summary(cmc, c, WORKLOADS["config4"], sms, max_mhz,
+                                                                    name="config4")),
                              ("sweep", lambda c: sweep_measure(cmc, c, args.sweep_trials)),
                              ("serve", lambda c: serve_measure(cmc, c, args))):
                 c2 = cmc.Context(local)

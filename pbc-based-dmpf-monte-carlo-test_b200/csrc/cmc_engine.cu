@@ -192,6 +192,35 @@ __device__ __forceinline__ uint32_t claim(uint32_t* counter, bool need, uint32_t
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// Per-trial PRP key schedule (cuckoo_bench.cu:226-232): the "KEY1" block of
+// the trial's offset under the batch key, expanded into gh->rk.
+__device__ __forceinline__ void trial_key(const Lanes& L, const Job& J, GroupHeader* gh) {
+    uint32_t w[4];
+    encrypt_full(L, J.batch_rk, 0x4b455931u, 0, gh->offset, 0x50525031u, w);
+    expand_key(L, w[0], w[1], w[2], w[3], gh->rk);
+}
+
+// Per-trial walk seed and affine input map (cuckoo_bench.cu:233-238): the
+// "WALK" block of the trial's offset under the batch key.
+__device__ __forceinline__ void trial_walk_seed(const Lanes& L, const Job& J, GroupHeader* gh) {
+    uint32_t w[4];
+    encrypt_full(L, J.batch_rk, 0x57414c4bu, 0, gh->offset, 0x524e4731u, w);
+    uint64_t walk = ((uint64_t)w[0] << 32) | w[1];
+    const uint64_t shift = (((uint64_t)w[2] << 32) | w[3]) & J.range_mask;
+    uint64_t input_state = shift ^ 0xd1b54a32d192ed03ULL;
+    gh->step = (splitmix(input_state) | 1ULL) & J.range_mask;
+    gh->shift = shift;
+    gh->rnd = splitmix(walk);
+    gh->walk = walk;
+}
+
+// Round-1 constants of Feistel round r (r < 8) into the trial's header.
+__device__ __forceinline__ void store_round1(const Lanes& L, GroupHeader* gh, uint32_t r, uint32_t h) {
+    const Round1 c = round1_consts(L, gh->rk, r, h);
+    gh->r1[r][0] = c.c0; gh->r1[r][1] = c.w3hi; gh->r1[r][2] = c.c1;
+    gh->r1[r][3] = c.c2; gh->r1[r][4] = c.c3;
+}
+
 // ---------------------------------------------------------------- producer --
 
 template <typename MapT, bool WIDE>
@@ -484,17 +513,8 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
 
         // Per-trial PRP key and walk seed (cuckoo_bench.cu:226-238).
         if (gt == 0) {
-            uint32_t w[4];
-            encrypt_full(L, J.batch_rk, 0x4b455931u, 0, gh->offset, 0x50525031u, w);
-            expand_key(L, w[0], w[1], w[2], w[3], gh->rk);
-            encrypt_full(L, J.batch_rk, 0x57414c4bu, 0, gh->offset, 0x524e4731u, w);
-            uint64_t walk = ((uint64_t)w[0] << 32) | w[1];
-            const uint64_t shift = (((uint64_t)w[2] << 32) | w[3]) & J.range_mask;
-            uint64_t input_state = shift ^ 0xd1b54a32d192ed03ULL;
-            gh->step = (splitmix(input_state) | 1ULL) & J.range_mask;
-            gh->shift = shift;
-            gh->rnd = splitmix(walk);
-            gh->walk = walk;
+            trial_key(L, J, gh);
+            trial_walk_seed(L, J, gh);
             gh->cand_next = 0;
             // Claim a free slot (FREE -> FILLING).  In-CTA slots: any free
             // one, starting from this group's share of the pool.  Split
@@ -549,11 +569,7 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         PrpKey key;
         if constexpr (!WIDE) {
             prp_key_from_schedule(gh->rk, key);
-            if (gt < 8) {
-                const Round1 c = round1_consts(L, gh->rk, gt, J.half_bits);
-                gh->r1[gt][0] = c.c0; gh->r1[gt][1] = c.w3hi; gh->r1[gt][2] = c.c1;
-                gh->r1[gt][3] = c.c2; gh->r1[gt][4] = c.c3;
-            }
+            if (gt < 8) store_round1(L, gh, gt, J.half_bits);
             if (smem_cache || glob_cache) build_fold_table(L, key, gh, fold, J.half_bits, gt, gthreads);
         }
         group_sync(g, gthreads);
@@ -737,30 +753,16 @@ __device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem,
                 }
                 __syncwarp();
                 const Job& J = gh->jd;
-                // per-trial PRP key (lane 0) and walk seed (lane 1), cuckoo_bench.cu:226-238
+                // per-trial PRP key (lane 0) and walk seed (lane 1)
                 if (lane == 0) {
-                    uint32_t w[4];
-                    encrypt_full(L, J.batch_rk, 0x4b455931u, 0, gh->offset, 0x50525031u, w);
-                    expand_key(L, w[0], w[1], w[2], w[3], gh->rk);
+                    trial_key(L, J, gh);
                 } else if (lane == 1) {
-                    uint32_t w[4];
-                    encrypt_full(L, J.batch_rk, 0x57414c4bu, 0, gh->offset, 0x524e4731u, w);
-                    uint64_t walk = ((uint64_t)w[0] << 32) | w[1];
-                    const uint64_t sh = (((uint64_t)w[2] << 32) | w[3]) & J.range_mask;
-                    uint64_t input_state = sh ^ 0xd1b54a32d192ed03ULL;
-                    gh->step = (splitmix(input_state) | 1ULL) & J.range_mask;
-                    gh->shift = sh;
-                    gh->rnd = splitmix(walk);
-                    gh->walk = walk;
+                    trial_walk_seed(L, J, gh);
                     gh->cand_next = 0;
                     gh->done = 0;
                 }
                 __syncwarp();
-                if (lane < 8) {
-                    const Round1 rc = round1_consts(L, gh->rk, lane, J.half_bits);
-                    gh->r1[lane][0] = rc.c0; gh->r1[lane][1] = rc.w3hi; gh->r1[lane][2] = rc.c1;
-                    gh->r1[lane][3] = rc.c2; gh->r1[lane][4] = rc.c3;
-                }
+                if (lane < 8) store_round1(L, gh, lane, J.half_bits);
                 __syncwarp();
                 if (lane == 0) gh->live = 1;
                 __syncwarp();
