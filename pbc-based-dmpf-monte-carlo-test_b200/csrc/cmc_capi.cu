@@ -128,9 +128,10 @@ int Ctx::make_job(const cmc_params& p, uint32_t first, uint32_t count, uint64_t 
 // Choose groups, warps per group and slot placement for a set of jobs.
 int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     uint32_t max_b = 0, max_cand = 0, max_cache_h = 0, any_cache = 0, wide = 0, wide_domain = 0;
-    uint32_t max_gcache_h = 0, any_gcache = 0;
+    uint32_t max_gcache_h = 0, any_gcache = 0, max_h = 0;
     double work = 0, cand_work = 0;
     for (const Job& j : jobs) {
+        max_h = std::max(max_h, j.half_bits);
         max_b = std::max(max_b, j.buckets);
         max_cand = std::max(max_cand, j.pnum * j.k);
         if (j.method == kMethodCache) {
@@ -184,10 +185,14 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     // headers and staged maps.  Dropped below if the walk slots go global.
     // Measured on B200 (same failure lists): t=64, B=96 24.4 -> 29.1 M
     // trials/s; t=27 42.3 -> 58.1 M; t=93 sequential 18.3 -> 20.7 M.
-    pl.pool_stage = 0;
+    // With h <= 10 the passes also take the round-2 fold (a trial's fold table
+    // has at most 4 entries per round, so a warp's fold loads touch few
+    // addresses): 111 table lookups per AES block instead of 124.
+    pl.pool_stage = pl.pool_fold = 0;
     if (force_pool != 0 && !any_cache && !any_gcache && !wide_domain && pl.wg == 1 && !pl.walker_ctas) {
         pl.pool_stage = round_up(max_cand * entry, 16);
-        pl.group_bytes = std::max(pl.group_bytes, pool_group_bytes(pl.pool_stage));
+        pl.pool_fold = max_h <= 10 ? fold_table_bytes(max_h) : 0;
+        pl.group_bytes = std::max(pl.group_bytes, pool_group_bytes(pl.pool_stage, pl.pool_fold));
     }
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
     auto groups_for = [&](uint32_t nw) {
@@ -250,7 +255,7 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
             pl.ns = ns_g;
         }
     }
-    if (!pl.slots_smem) pl.pool_stage = 0;
+    if (!pl.slots_smem) pl.pool_stage = pl.pool_fold = 0;
     pl.group_off = kEngineTableBytes + kCtaSharedBytes;
     pl.slots_off = pl.group_off + pl.ng * pl.group_bytes;
     pl.smem_bytes = pl.slots_off + (pl.slots_smem ? pl.ns * pl.slot_stride : 0);
@@ -380,6 +385,7 @@ int Ctx::run(const std::vector<Job>& jobs, uint64_t total, cudaStream_t st, uint
         a.map_chains = map_chains;
         a.fill_blocks = fill_blocks;
         a.pool_stage = pl.pool_stage;
+        a.pool_fold = pl.pool_fold;
         return a;
     };
     // Fused: one launch per entry width that two or more classes share (the

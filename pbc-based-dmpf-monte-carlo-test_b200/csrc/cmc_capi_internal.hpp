@@ -27,6 +27,7 @@ struct Plan {
     uint32_t gcache_stride = 0;   // u16 entries per group's global round cache
     uint64_t gcache_bytes = 0;    // all groups' global round caches
     uint32_t pool_stage = 0;      // pooled direct passes: bytes per staging map (0: off)
+    uint32_t pool_fold = 0;       // pooled direct passes: bytes per fold table (0: unfolded)
 };
 
 uint32_t choose_method(uint32_t h, uint64_t domain, double candidates, int force, bool may_allocate);

@@ -659,6 +659,10 @@ __device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem,
     auto stage = [&](uint32_t j) {
         return reinterpret_cast<MapT*>(gbase + kPoolContexts * kPoolHeaderStride + j * a.pool_stage);
     };
+    auto fold = [&](uint32_t j) {
+        return reinterpret_cast<uint4*>(gbase + kPoolContexts * (kPoolHeaderStride + a.pool_stage) +
+                                        j * a.pool_fold);
+    };
     const unsigned long long total = a.total_dev ? *a.total_dev : a.total;
     if (lane < kPoolContexts) ctx(lane)->live = 0;
     __syncwarp();
@@ -670,6 +674,23 @@ __device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem,
     uint32_t h = 0, mask = 0, kk = 0, width = 0, wmagic = 0, c = 0, l = 0, r = 0;
     uint64_t domain = 0, shift = 0, step = 0, rmask = 0;
     bool sequential = false;
+    // take context j's key and parameters
+    auto bind = [&](uint32_t j) {
+        const GroupHeader* gh = ctx(j);
+        const Job& J = gh->jd;
+        prp_key_from_schedule(gh->rk, key);
+        h = J.half_bits;
+        mask = (uint32_t)J.mask;
+        domain = J.domain;
+        kk = J.k;
+        width = (uint32_t)J.width;
+        wmagic = J.width_magic;
+        sequential = J.input_mode == 0;
+        shift = gh->shift;
+        step = gh->step;
+        rmask = J.range_mask;
+        kj = (int)j;
+    };
     for (;;) {
         // converged: publish finished trials, start new ones
 #pragma unroll 1
@@ -764,6 +785,18 @@ __device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem,
                 __syncwarp();
                 if (lane < 8) store_round1(L, gh, lane, J.half_bits);
                 __syncwarp();
+                if (a.pool_fold) {
+                    // the trial's round-2 fold table (fold_entry in cmc_aes.cuh),
+                    // built with its key; lanes take their own trial's key back
+                    // before their next pass
+                    prp_key_from_schedule(gh->rk, key);
+                    kj = -1;
+                    const uint32_t yb = J.half_bits > 8 ? J.half_bits - 8 : 0;
+                    uint4* fd = fold(j);
+                    for (uint32_t v = lane; v < (8u << yb); v += 32)
+                        fd[v] = fold_entry(L, key, load_round1(gh, v >> yb), v & ((1u << yb) - 1u));
+                    __syncwarp();
+                }
                 if (lane == 0) gh->live = 1;
                 __syncwarp();
             }
@@ -781,21 +814,7 @@ __device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem,
             if (need && nc < gh->jd.pnum * gh->jd.k) {
                 cj = (int)j;
                 c = nc;
-                if (kj != (int)j) {
-                    const Job& J = gh->jd;
-                    prp_key_from_schedule(gh->rk, key);
-                    h = J.half_bits;
-                    mask = (uint32_t)J.mask;
-                    domain = J.domain;
-                    kk = J.k;
-                    width = (uint32_t)J.width;
-                    wmagic = J.width_magic;
-                    sequential = J.input_mode == 0;
-                    shift = gh->shift;
-                    step = gh->step;
-                    rmask = J.range_mask;
-                    kj = (int)j;
-                }
+                if (kj != (int)j) bind(j);
                 const uint32_t o = div_k(c, kk), jc = c - o * kk;
                 const uint64_t e = sequential ? (uint64_t)o : (shift + (uint64_t)o * step) & rmask;
                 const uint32_t y = (uint32_t)(e * kk + jc);
@@ -805,14 +824,29 @@ __device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem,
         }
         // one Feistel pass (8 rounds) per lane with a candidate
         if (cj >= 0) {
+            if (kj != cj) bind((uint32_t)cj);
             const GroupHeader* gh = ctx((uint32_t)cj);
+            if (a.pool_fold) {
+                // rounds 1-2 from the fold table: entry (rr, R >> 8)
+                const uint4* fd = fold((uint32_t)cj);
+                const uint32_t yb = h > 8 ? h - 8 : 0;
 #pragma unroll 1
-            for (uint32_t rr = 0; rr < 8; ++rr) {
-                const Round1 rc = load_round1(gh, rr);
-                const uint32_t f = prp_f(L, key, rc, r) & mask;
-                const uint32_t nr = (l ^ f) & mask;
-                l = r;
-                r = nr;
+                for (uint32_t rr = 0; rr < 8; ++rr) {
+                    const uint2 k01 = *reinterpret_cast<const uint2*>(&gh->r1[rr][0]);
+                    const uint32_t f = prp_f_folded(L, key, k01.x, k01.y, fd[(rr << yb) | (r >> 8)], r) & mask;
+                    const uint32_t nr = (l ^ f) & mask;
+                    l = r;
+                    r = nr;
+                }
+            } else {
+#pragma unroll 1
+                for (uint32_t rr = 0; rr < 8; ++rr) {
+                    const Round1 rc = load_round1(gh, rr);
+                    const uint32_t f = prp_f(L, key, rc, r) & mask;
+                    const uint32_t nr = (l ^ f) & mask;
+                    l = r;
+                    r = nr;
+                }
             }
             const uint32_t y = (l << h) | r;
             if (y < domain) {

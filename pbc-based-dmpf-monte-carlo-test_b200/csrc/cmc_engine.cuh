@@ -22,11 +22,12 @@ constexpr uint32_t kGroupHeaderBytes = 1024;  // per-group shared header (the tr
 // Pooled direct passes (EngineArgs::pool_stage != 0): a one-warp group keeps
 // kPoolContexts trials in flight, each with its own header (kPoolHeaderStride
 // apart: 16 bytes more than a header, so the contexts' round constants fall in
-// different banks) and a staging map of pool_stage bytes after the headers.
+// different banks), a staging map of pool_stage bytes after the headers, and,
+// when pool_fold != 0, a round-2 fold table of pool_fold bytes after those.
 constexpr uint32_t kPoolContexts = 3;  // measured: 2 and 3 within 0.3 % at t=64, 3 +5 % at t=27; 4 slower
 constexpr uint32_t kPoolHeaderStride = kGroupHeaderBytes + 16;
-__host__ __device__ constexpr uint32_t pool_group_bytes(uint32_t stage) {
-    return kPoolContexts * (kPoolHeaderStride + stage);
+__host__ __device__ constexpr uint32_t pool_group_bytes(uint32_t stage, uint32_t fold) {
+    return kPoolContexts * (kPoolHeaderStride + stage + fold);
 }
 
 // A group's shared region: [header, kGroupHeaderBytes][round-2 fold table of a
@@ -133,6 +134,7 @@ struct EngineArgs {
     uint32_t map_chains;                // lookup chains per lane from a round cache (0: automatic)
     uint32_t fill_blocks;               // round-cache fill: blocks per thread per step (0: automatic)
     uint32_t pool_stage;                // pooled direct passes: bytes per staging map (0: off)
+    uint32_t pool_fold;                 // pooled direct passes: bytes per fold table (0: unfolded)
     unsigned long long entry_begin;
     unsigned long long bits_mask;
     unsigned int* entry_done;

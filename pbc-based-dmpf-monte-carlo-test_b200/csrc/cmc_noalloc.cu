@@ -205,6 +205,7 @@ extern "C" int cmc_launch_static(const cmc_params* params, const uint32_t* d_bat
     a.spin_limit = pl_ctx.spin_limit;
     a.idle_polls = pl_ctx.spin_limit;
     a.pool_stage = pl.pool_stage;
+    a.pool_fold = pl.pool_fold;
     // walk slots in shared memory (checked above)
     const void* fn = engine_kernel(pl.variant, true, pl.pool_stage != 0);
     // the engine's shared-memory limit was raised to the device maximum at set-up

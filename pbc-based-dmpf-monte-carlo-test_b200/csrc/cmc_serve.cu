@@ -658,6 +658,7 @@ struct Server {
         a.map_chains = ctx->map_chains;
         a.fill_blocks = ctx->fill_blocks;
         a.pool_stage = pl.pool_stage;
+        a.pool_fold = pl.pool_fold;
         const void* fn = engine_kernel(pl.variant, pl.slots_smem, pl.pool_stage != 0);
         // the context raised the engine's shared-memory limit to the device maximum
         void* args[] = {&a};

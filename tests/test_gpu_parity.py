@@ -201,10 +201,14 @@ def test_full_batch_properties(ctx, cmc):
     ("bgh25", "sequential", 27, 12, 2, 30, 5),
     ("bgh25", "affine", 300, 20, 4, 330, 50),
     ("drrt18", "sequential", 5, 8, 3, 6, 5),       # fewer candidates than lanes
+    ("bgh25", "affine", 100, 18, 3, 130, 100),     # h = 10: 4 fold entries per round
+    ("bgh25", "affine", 40, 17, 2, 50, 30),        # h = 10, k = 2
 ])
 def test_pooled_direct_passes_vs_oracle(ctx, cmc, oracle, shape):
     # three trials in flight per one-warp group, maps staged and copied into
-    # slots at publish time: every trial's outcome as the oracle has it
+    # slots at publish time, rounds 1-2 from the trial's fold table when
+    # h <= 10 (the t = 300 shape, h = 11, takes unfolded passes): every
+    # trial's outcome as the oracle has it
     mode, im, pnum, ell, k, buckets, kick = shape
     apply(ctx, {"pool": 1, "warps_per_group": 1, "method": 0})
     p = cmc.parameters(mode, pnum, ell, k, buckets, kick, im)

@@ -13,7 +13,7 @@ SHAPES = [
     ("config2", ("bgh25", 1024, 20, 3, 1536, 500, "affine"), 2, 1 << 18, {}, 3.47e6),
     ("config2_global_slots", ("bgh25", 1024, 20, 3, 1536, 500, "affine"), 2, 1 << 18,
      {"warps_per_group": 3, "groups": 4}, 3.44e6),
-    ("config1", ("bgh25", 64, 16, 3, 96, 100, "affine"), 1, 1 << 20, {}, 2.75e7),
+    ("config1", ("bgh25", 64, 16, 3, 96, 100, "affine"), 1, 1 << 20, {}, 3.0e7),
     ("config4", ("bgh25", 16384, 28, 3, 24576, 1000, "affine"), 4, 1 << 16, {}, 1.62e5),
     ("t8000_global_slots", ("bgh25", 8000, 24, 3, 11200, 500, "affine"), 5, 1 << 16, {}, 4.2e5),
 ]
