@@ -649,7 +649,9 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
 // takes one from the next, loading that trial's key when it switches, and a
 // finished trial is published (its staged map copied into a free slot) and
 // replaced by the next one at the top of the loop, where the warp is
-// converged.  A slot is held only while its map is copied.
+// converged.  A slot is held only while its map is copied.  With pool_fold
+// set (h <= 10), rounds 1-2 of every pass come from the trial's round-2 fold
+// table (fold_entry in cmc_aes.cuh), built when the trial starts.
 template <typename MapT, typename BinT>
 __device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem, CtaShared* cs, uint32_t g,
                                                 uint32_t lane) {
