@@ -128,10 +128,14 @@ int Ctx::make_job(const cmc_params& p, uint32_t first, uint32_t count, uint64_t 
 // Choose groups, warps per group and slot placement for a set of jobs.
 int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     uint32_t max_b = 0, max_cand = 0, max_cache_h = 0, any_cache = 0, wide = 0, wide_domain = 0;
-    uint32_t max_gcache_h = 0, any_gcache = 0, max_h = 0;
+    uint32_t max_gcache_h = 0, any_gcache = 0, max_h = 0, dfold_h = 0, any_dfold = 0;
     double work = 0, cand_work = 0;
     for (const Job& j : jobs) {
         max_h = std::max(max_h, j.half_bits);
+        if (!plan_no_dfold && j.method == kMethodDirect && j.domain <= 0xffffffffULL && j.half_bits <= 13) {
+            any_dfold = 1;  // direct passes with a word-split round-2 fold table
+            dfold_h = std::max(dfold_h, j.half_bits);
+        }
         max_b = std::max(max_b, j.buckets);
         max_cand = std::max(max_cand, j.pnum * j.k);
         if (j.method == kMethodCache) {
@@ -159,7 +163,8 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     // its group's shared region
     const uint32_t cache_bytes = any_cache ? fold_table_bytes(max_cache_h) + (16u << max_cache_h) : 0;
     const uint32_t gfold_bytes = any_gcache ? fold_table_bytes(max_gcache_h) : 0;
-    pl.group_bytes = kGroupHeaderBytes + std::max(cache_bytes, gfold_bytes);
+    const uint32_t dfold_bytes = any_dfold ? fold_table_bytes(dfold_h) : 0;
+    pl.group_bytes = kGroupHeaderBytes + std::max({cache_bytes, gfold_bytes, dfold_bytes});
     const double avg_cand = work > 0 ? cand_work / work : 0;
     // one-warp groups for direct passes up to 1,536 candidates per trial (with
     // pooled passes, measured: t=300 k=3 6.75 M trials/s against 5.14 M in
@@ -192,7 +197,7 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
     if (force_pool != 0 && !any_cache && !any_gcache && !wide_domain && pl.wg == 1 && !pl.walker_ctas) {
         pl.pool_stage = round_up(max_cand * entry, 16);
         pl.pool_fold = max_h <= 10 ? fold_table_bytes(max_h) : 0;
-        pl.group_bytes = std::max(pl.group_bytes, pool_group_bytes(pl.pool_stage, pl.pool_fold));
+        pl.group_bytes = pool_group_bytes(pl.pool_stage, pl.pool_fold);  // its own fold, if any
     }
     const uint32_t budget = uint32_t(smem_optin) - kEngineTableBytes - kCtaSharedBytes;
     auto groups_for = [&](uint32_t nw) {
@@ -280,6 +285,17 @@ int Ctx::plan(const std::vector<Job>& jobs, Plan& pl) {
              any_cache && any_gcache ? "smem+global" : any_cache ? "smem" : any_gcache ? "global" : "off",
              pl.pool_stage ? " pooled" : "");
     plan_text = buf;
+    // The fold tables of direct passes (build_map_direct) come out of the walk
+    // slots' shared memory; with fewer than 4 slots per group left, or none,
+    // the walks lose more than the passes gain (measured at t=2000, h=13:
+    // 9 -> 6 slots, 0.82 -> 0.72 M trials/s; t=1000: 18 -> 15 slots, 1.59 ->
+    // 1.74 M), so plan again without them.
+    if (any_dfold && !pl.pool_stage && (!pl.slots_smem || pl.ns < 4 * pl.ng)) {
+        plan_no_dfold = true;
+        const int rc2 = plan(jobs, pl);
+        plan_no_dfold = false;
+        return rc2;
+    }
     return CMC_OK;
 }
 

@@ -100,6 +100,7 @@ struct Ctx {
     std::string graph_state;                 // "eager", "captured" or "replayed"
     int force_method = -1;  // -1 auto, 0 direct, 1 cache (shared if h <= 12, else global), 2 global cache
     int force_pool = -1;    // pooled direct passes: -1 auto, 0 off, 1 on where they apply
+    bool plan_no_dfold = false;  // plan() re-run without room for direct passes' fold tables
     bool may_allocate = true;  // false: no global round cache, global slots only if unavoidable
     uint32_t spin_limit = 1u << 26;
     uint32_t map_chains = 0;  // lookup chains per lane from a round cache (0: automatic)

@@ -223,9 +223,15 @@ __device__ __forceinline__ void store_round1(const Lanes& L, GroupHeader* gh, ui
 
 // ---------------------------------------------------------------- producer --
 
-template <typename MapT, bool WIDE>
+// FOLD: rounds 1-2 of each pass from the trial's round-2 fold table, kept
+// word-split (component c of entry v at fw[c * n + v], n = 8 << yb) so that a
+// warp's loads of one component are conflict-free while a round has at most
+// 32 entries (h <= 13): 111 table lookups and 4 fold loads per block instead
+// of 124 lookups.
+template <typename MapT, bool WIDE, bool FOLD = false>
 __device__ __forceinline__ void build_map_direct(const Lanes& L, const Job& J, GroupHeader* gh,
-                                                 const PrpKey& key, MapT* map, uint32_t lane) {
+                                                 const PrpKey& key, MapT* map, uint32_t lane,
+                                                 const uint32_t* fw = nullptr) {
     const uint32_t k = J.k, ncand = J.pnum * k, h = J.half_bits;
     const uint64_t mask = J.mask, domain = J.domain;
     const bool sequential = J.input_mode == 0;
@@ -244,13 +250,27 @@ __device__ __forceinline__ void build_map_direct(const Lanes& L, const Job& J, G
     while (__any_sync(kFull, has)) {
         if constexpr (!WIDE) {
             uint32_t l = (uint32_t)left, r = (uint32_t)right;
+            if constexpr (FOLD) {
+                const uint32_t yb = h > 8 ? h - 8 : 0, n = 8u << yb;
 #pragma unroll 1
-            for (uint32_t rr = 0; rr < 8; ++rr) {
-                const Round1 rc = load_round1(gh, rr);
-                const uint32_t f = prp_f(L, key, rc, r) & (uint32_t)mask;
-                const uint32_t nr = (l ^ f) & (uint32_t)mask;
-                l = r;
-                r = nr;
+                for (uint32_t rr = 0; rr < 8; ++rr) {
+                    const uint2 k01 = *reinterpret_cast<const uint2*>(&gh->r1[rr][0]);
+                    const uint32_t vi = (rr << yb) | (r >> 8);
+                    const uint4 v = make_uint4(fw[vi], fw[n + vi], fw[2 * n + vi], fw[3 * n + vi]);
+                    const uint32_t f = prp_f_folded(L, key, k01.x, k01.y, v, r) & (uint32_t)mask;
+                    const uint32_t nr = (l ^ f) & (uint32_t)mask;
+                    l = r;
+                    r = nr;
+                }
+            } else {
+#pragma unroll 1
+                for (uint32_t rr = 0; rr < 8; ++rr) {
+                    const Round1 rc = load_round1(gh, rr);
+                    const uint32_t f = prp_f(L, key, rc, r) & (uint32_t)mask;
+                    const uint32_t nr = (l ^ f) & (uint32_t)mask;
+                    l = r;
+                    r = nr;
+                }
             }
             left = l;
             right = r;
@@ -418,6 +438,22 @@ __device__ __forceinline__ void build_fold_table(const Lanes& L, const PrpKey& k
     }
 }
 
+// The same table word-split, for direct passes (build_map_direct<..., true>).
+__device__ __forceinline__ void build_fold_table_split(const Lanes& L, const PrpKey& key,
+                                                       const GroupHeader* gh, uint32_t* fw, uint32_t h,
+                                                       uint32_t gt, uint32_t gthreads) {
+    const uint32_t yb = h > 8 ? h - 8 : 0;
+    const uint32_t n = 8u << yb;
+    for (uint32_t v = gt; v < n; v += gthreads) {
+        const Round1 c = round1_consts(L, gh->rk, v >> yb, h);
+        const uint4 e = fold_entry(L, key, c, v & ((1u << yb) - 1u));
+        fw[v] = e.x;
+        fw[n + v] = e.y;
+        fw[2 * n + v] = e.z;
+        fw[3 * n + v] = e.w;
+    }
+}
+
 template <typename MapT, typename BinT, bool WIDE, bool SPLIT, bool SMEMSLOTS>
 __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaShared* cs, uint32_t g,
                                          uint32_t gt) {
@@ -565,12 +601,22 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
         const bool glob_cache = !WIDE && !smem_cache && J.method == kMethodGCache &&
                                 a.gcache != nullptr && cache_entries <= a.gcache_stride &&
                                 fold_end <= a.group_bytes;
+        // direct passes take the fold too, in the shared-slot kernels (the
+        // global-slot kernels are left as they are: their walks are sensitive
+        // to the kernel's register allocation, cmc_engine below)
+        const bool direct_fold = SMEMSLOTS && !WIDE && J.method == kMethodDirect && J.half_bits <= 13 &&
+                                 fold_end <= a.group_bytes;
         uint4* fold = reinterpret_cast<uint4*>(gbase + kGroupHeaderBytes);
         PrpKey key;
         if constexpr (!WIDE) {
             prp_key_from_schedule(gh->rk, key);
             if (gt < 8) store_round1(L, gh, gt, J.half_bits);
             if (smem_cache || glob_cache) build_fold_table(L, key, gh, fold, J.half_bits, gt, gthreads);
+            if constexpr (SMEMSLOTS) {
+                if (direct_fold)
+                    build_fold_table_split(L, key, gh, reinterpret_cast<uint32_t*>(fold), J.half_bits, gt,
+                                           gthreads);
+            }
         }
         group_sync(g, gthreads);
 
@@ -601,6 +647,9 @@ __device__ __forceinline__ void producer(const EngineArgs& a, char* smem, CtaSha
             // the overlap gains (measured: t=1500, k=4, c~4: 4 chains 8% slower)
             const bool light_walk = (1ULL << (2 * J.half_bits)) <= 2 * J.domain;
             map_from_cache<MapT>(J, gh, gc, map, lane, a.map_chains ? a.map_chains : (light_walk ? 4 : 2));
+        } else if (SMEMSLOTS && !WIDE && direct_fold) {
+            build_map_direct<MapT, WIDE, SMEMSLOTS && !WIDE>(L, J, gh, key, map, lane,
+                                                             reinterpret_cast<const uint32_t*>(fold));
         } else {
             build_map_direct<MapT, WIDE>(L, J, gh, key, map, lane);
         }

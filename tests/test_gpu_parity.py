@@ -218,3 +218,21 @@ def test_pooled_direct_passes_vs_oracle(ctx, cmc, oracle, shape):
     assert "pooled" in ctx.last_plan, ctx.last_plan
     assert got == want, (shape, ctx.last_plan)
 
+
+@pytest.mark.parametrize("shape", [
+    # mode, input, t, ell_i, k, B, kick: direct passes in 4-warp groups with
+    # shared walk slots, rounds 1-2 from the word-split fold table (h <= 13)
+    ("bgh25", "affine", 1000, 24, 3, 1300, 200),   # h = 13: 32 fold entries per round
+    ("drrt18", "sequential", 800, 20, 3, 1000, 50),
+    ("bgh25", "affine", 700, 24, 4, 900, 500),      # h = 14: unfolded passes
+])
+def test_folded_direct_passes_vs_oracle(ctx, cmc, oracle, shape):
+    mode, im, pnum, ell, k, buckets, kick = shape
+    apply(ctx, {"method": 0, "warps_per_group": 4, "groups": 3, "pool": 0})
+    p = cmc.parameters(mode, pnum, ell, k, buckets, kick, im)
+    op = oracle.params(mode, pnum, ell, k, buckets, kick, im)
+    want = oracle.batch(op, 13, 1, 7, 200)
+    got = ctx.launch(p, cmc.batch_key(13, 1), 7, 200)
+    assert "slots_in=smem" in ctx.last_plan, ctx.last_plan
+    assert got == want, (shape, ctx.last_plan)
+
