@@ -803,18 +803,20 @@ __device__ __forceinline__ void producer_pooled(const EngineArgs& a, char* smem,
                 __syncwarp();
             }
             if (!gh->live && more) {
+                uint32_t claimed = 0;  // the claim holds a trial
                 if (lane == 0) {
                     const unsigned long long gi = a.gidx_begin + atomicAdd(&a.ctrl->next, 1ULL);
                     gh->gidx = gi;
-                    gh->abort = gi < total;  // here: the claim holds a trial
-                    if (gi < total) {
+                    claimed = gi < total;
+                    if (claimed) {
                         const uint32_t jb = find_job(a.jobs, a.njobs, gi);
                         gh->job = jb;
                         gh->offset = a.jobs[jb].first + (uint32_t)(gi - a.jobs[jb].trial_base);
                     }
                 }
+                claimed = __shfl_sync(kFull, claimed, 0);
                 __syncwarp();
-                if (!gh->abort) {
+                if (!claimed) {
                     more = false;
                     continue;
                 }
