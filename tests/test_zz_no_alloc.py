@@ -16,6 +16,8 @@ SHAPES = {
     # 32-bit entries (the other 32-bit-entry shapes, B > 65535 or t > 16384,
     # never fit shared-memory slots and are rejected below)
     "wide_domain": (("drrt18", 40, 33, 3, 48, 20, "affine"), 5, 512),
+    # one-warp groups with pooled, folded direct passes (cmc_engine_pooled)
+    "pooled": (("bgh25", 64, 16, 3, 70, 20, "affine"), 3, 8192),
 }
 
 
